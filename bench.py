@@ -1,0 +1,403 @@
+#!/usr/bin/env python
+"""UMAP layout throughput on B200: edge-updates/s at 1M points.
+
+One step = one full layout run (all epochs) of one embedding problem from its
+cached fuzzy graph, the unit the reference's timing harness isolates
+(tests/umap_gpu_bench.rs:217-252). An edge-update is one active undirected
+edge in one epoch (cursor <= epoch), both endpoints' attractive and negative
+terms included; the count per epoch depends only on the edge periods, so it
+is the same for every implementation.
+
+  value  : device-resident state (graph, embedding, moments on the GPU),
+           CUDA events around the epoch loop on the launching stream,
+           L2 flushed (256 MiB write) before every step.
+  e2e    : the reference-facing call umapcu.optimise_embedding_adam_gpu
+           (C ABI umapcu_optimise_embedding) from pinned host buffers:
+           H2D of graph + embedding, CSR build, epochs, D2H of the embedding.
+  --impl reference : the reference's parallel Adam (umap_optimisers.rs:
+           1170-1492, restated in oracle/) on the host cores, bounded windows.
+
+Multi-GPU (torchrun): every rank runs its own problem (replicas, seed +
+rank); value is the sum over ranks / max-over-ranks time ("weak").
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (ROOT, os.path.join(ROOT, "manifolds-rs_b200")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "UMAP layout edge-updates/s (1M pts)"
+UNIT = "edge-updates/s"
+
+WORKLOADS = {
+    "c2": dict(n=1_000_000, dim=50, clusters=30, k=15, n_epochs=200, kind="anisotropic", dens=False,
+               desc="1M x 50 f32, 30-component anisotropic Gaussian mixture (eig log-U[0.1,4], Dirichlet(1) "
+                    "weights), exact kNN k=15 cached, 2-D, 200 epochs, Adam, neg_rate 5, random U(-10,10) init"),
+    "c1": dict(n=10_000, dim=50, clusters=10, k=15, n_epochs=500, kind="isotropic", dens=False,
+               desc="10k x 50 f32, 10 isotropic Gaussians, exact kNN k=15, 2-D, 500 epochs, Adam, neg_rate 5"),
+    "c3": dict(n=200_000, dim=30, clusters=20, k=30, n_epochs=200, kind="variable", dens=True,
+               desc="densMAP 200k x 30 f32, 20 clusters sd log-U[0.2,3], k=30, 2-D, 200 epochs, last 30% "
+                    "density term, lambda 2, Adam"),
+}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ----------------------------------------------------------------- inputs
+
+def make_problem(wl, seed, device_knn=True, reference_graph=False):
+    """Synthetic data -> exact kNN (torch on the GPU: input preparation) ->
+    fuzzy graph: the CUDA graph stage for the umapcu arm, the oracle's CPU
+    restatement of the reference's graph stage for the reference arm."""
+    import umapcu
+    import umapcu.synth as S
+    t0 = time.time()
+    if wl["kind"] == "anisotropic":
+        X, _ = S.anisotropic_mixture(wl["n"], wl["dim"], wl["clusters"], seed)
+    elif wl["kind"] == "variable":
+        X, _ = S.variable_density_mixture(wl["n"], wl["dim"], wl["clusters"], seed)
+    else:
+        X, _ = S.isotropic_mixture(wl["n"], wl["dim"], wl["clusters"], seed)
+    idx, dist = S.exact_knn_torch(X, wl["k"]) if device_knn else S.exact_knn_cpu(X, wl["k"])
+    t1 = time.time()
+    if reference_graph:
+        from oracle import oracle as O
+        (r, c, v), _, _ = O.construct_umap_graph(idx, dist, wl["n_epochs"])
+        graph = umapcu.CoordinateList(r, c, v, wl["n"])
+        dens = None
+        if wl["dens"]:
+            stt, d = O.dens_state_new(wl["n"], r, c, v, idx, dist, True)
+            dens = umapcu.DensState(umapcu.DensParams(), d["r"], d["mu_sum"], float(d["mu_tot"]))
+    else:
+        graph = umapcu.construct_umap_graph(idx, dist, umapcu.UmapGraphParams(), wl["n_epochs"])
+        dens = umapcu.DensState.new(umapcu.DensParams(), graph, idx, dist, True) if wl["dens"] else None
+    adj = umapcu.coo_to_adjacency_list(graph)
+    params = umapcu.UmapOptimParams.from_min_dist_spread(0.1, 1.0, n_epochs=wl["n_epochs"], neg_sample_rate=5)
+    init = umapcu.random_layout(wl["n"], 2, seed)
+    log(f"[bench] data+kNN {t1 - t0:.1f}s, graph {time.time() - t1:.1f}s, nnz {adj.col.size}")
+    return dict(X=X, idx=idx, dist=dist, graph=graph, adj=adj, dens=dens, params=params, init=init)
+
+
+def active_edges_per_epoch(eps, n_epochs):
+    """A_e: edges with cursor <= e under the f32 schedule of
+    umap_optimiser_gpu.rs:741/952 (cursor starts at the period)."""
+    eps = np.asarray(eps, np.float32)
+    cur = eps.copy()
+    out = np.zeros(n_epochs, np.int64)
+    for e in range(n_epochs):
+        act = cur <= np.float32(e)
+        out[e] = int(act.sum())
+        cur[act] += eps[act]
+    return out
+
+
+# ----------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.dev)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, ValueError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------- CPU leg
+
+def cpu_windows(prob, wl, seed, target_s, n_threads):
+    """Times the oracle's adam_parallel on bounded mid-run windows of the
+    same workload; returns (edge-updates/s, sample description, cores)."""
+    from oracle import oracle as O
+    p = prob["params"].as_dict()
+    adj = prob["adj"]
+    dens = None
+    if prob["dens"] is not None:
+        d = prob["dens"]
+        dens = {"r": d.r, "lambda": d.params.lambda_, "frac": d.params.frac, "var_shift": d.params.var_shift,
+                "mu_tot": d.mu_tot}
+    n = wl["n"]
+    ae = prob["A_e"]
+    first = wl["n_epochs"] // 2
+    # calibrate on one epoch, then size the window to ~target_s
+    st, _, s1 = O.optimise_adam_parallel(prob["init"], n, adj.ptr, adj.col, adj.w, p, seed, dens, n_threads, 1,
+                                         first, True)
+    per = max(s1, 1e-3)
+    cnt = int(max(1, min(wl["n_epochs"] - first, round(target_s / per))))
+    st, _, secs = O.optimise_adam_parallel(prob["init"], n, adj.ptr, adj.col, adj.w, p, seed, dens, n_threads, cnt,
+                                           first, True)
+    updates = int(ae[first:first + cnt].sum())
+    return updates / secs, f"epochs {first}..{first + cnt - 1} of the {wl['n_epochs']}-epoch run " \
+                           f"({updates} edge-updates, {secs:.2f}s)", secs
+
+
+# ----------------------------------------------------------------- main
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="umapcu", choices=["umapcu", "reference"])
+    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--sampler", default="ref_hash", choices=["ref_hash", "philox"])
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--cpu-seconds", type=float, default=8.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--profile-only", action="store_true", help="small run for ncu captures")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    wl = dict(WORKLOADS[args.workload])
+
+    import torch
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        run_reference(args, wl, world)
+        return
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    import umapcu
+    seed = args.seed + rank
+    prob = make_problem(wl, seed)
+    sampler = umapcu.NEG_PHILOX if args.sampler == "philox" else umapcu.NEG_REF_HASH
+    st = umapcu.UmapGpuState(prob["init"], prob["adj"], prob["params"], prob["dens"], seed, sampler)
+    E = st.n_edges
+    csr = st.csr()
+    ae = active_edges_per_epoch(csr["eps"], wl["n_epochs"])
+    prob["A_e"] = ae
+    updates_per_step = int(ae.sum())
+    n_ep = wl["n_epochs"]
+    stream = torch.cuda.current_stream()
+    st.set_stream(stream.cuda_stream)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > L2
+
+    if args.profile_only:
+        st.reset(prob["init"])
+        st.run(0, min(n_ep, 8))
+        torch.cuda.synchronize()
+        log("[bench] profile-only run done")
+        return
+
+    for _ in range(args.warmup):
+        st.reset(prob["init"])
+        st.run(0, n_ep)
+    torch.cuda.synchronize()
+
+    times = []
+    with ClockSampler(local_rank) as clk:
+        for _ in range(args.steps):
+            st.reset(prob["init"])
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            if dist:
+                dist.barrier()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            st.run(0, n_ep)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1) / 1e3)
+    total = float(np.sum(times))
+    if dist:
+        t = torch.tensor([total], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total = float(t.item())
+    value = world * args.steps * updates_per_step / total
+    ms_per_step = total / args.steps * 1e3
+
+    # roofline of the dominant kernel (fused epoch kernel), events per launch
+    st.reset(prob["init"])
+    torch.cuda.synchronize()
+    k_ms, d_ms = st.run_profiled(0, n_ep)
+    avg_launch_s = k_ms / 1e3 / n_ep
+    n_nodes = wl["n"]
+    nd = 2
+    alg_bytes = (112.0 * updates_per_step + n_ep * (8.0 * E) + 4.0 * updates_per_step
+                 + n_ep * n_nodes * nd * 4 * 7) / n_ep
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = alg_bytes / avg_launch_s / 1e9
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", f"k_epoch_{args.workload}_traffic.txt")
+    if os.path.exists(tf):
+        for ln in open(tf):
+            if ln.startswith("dram_bytes_per_launch:"):
+                traffic = float(ln.split(":")[1])
+    roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "traffic": traffic,
+            "kernel": "k_epoch<2,false>" if not wl["dens"] else "k_epoch<2,true>",
+            "avg_launch_us": round(avg_launch_s * 1e6, 2),
+            "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
+
+    # end to end through the reference-facing C-ABI call, pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        adj = prob["adj"]
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+        ptr_p, col_p, w_p = pin(adj.ptr), pin(adj.col), pin(adj.w)
+        embd_p = pin(prob["init"])
+        A = umapcu.Adjacency(ptr_p, col_p, w_p)
+        init = prob["init"]
+        e2e_steps = max(1, min(args.steps, 3))
+        for _ in range(1):
+            embd_p[...] = init
+            umapcu.optimise_embedding_adam_gpu(embd_p, A, prob["params"], prob["dens"], seed, 0, sampler)
+        tt = []
+        for _ in range(e2e_steps):
+            embd_p[...] = init
+            torch.cuda.synchronize()
+            if dist:
+                dist.barrier()
+            t0 = time.perf_counter()
+            umapcu.optimise_embedding_adam_gpu(embd_p, A, prob["params"], prob["dens"], seed, 0, sampler)
+            tt.append(time.perf_counter() - t0)
+        et = float(np.sum(tt))
+        if dist:
+            t = torch.tensor([et], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            et = float(t.item())
+        h2d = ptr_p.nbytes + col_p.nbytes + w_p.nbytes + embd_p.nbytes
+        e2e = {"value": world * e2e_steps * updates_per_step / et, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(embd_p.nbytes), "ms_per_step": round(et / e2e_steps * 1e3, 3)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        v, sample, secs = cpu_windows(prob, wl, seed, args.cpu_seconds, threads)
+        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
+
+    dens_launches = 0
+    if wl["dens"]:
+        dp = prob["dens"]
+        dens_launches = 4 * sum(1 for e in range(n_ep) if dp.is_active(e, n_ep))
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"{args.workload}: {wl['desc']}", "n_points": wl["n"], "n_edges": int(E),
+                       "edge_updates_per_step": updates_per_step, "epochs": n_ep,
+                       "sampler": args.sampler, "l2": "flushed before every step (256 MiB write)",
+                       "parallelism": f"replicas x{world}"},
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": args.steps * (n_ep + dens_launches),
+            "clocks": clk.summary(),
+            "densmap_ms_per_step": round(d_ms, 3) if wl["dens"] else None,
+        }
+        print(json.dumps(out), flush=True)
+    st.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_reference(args, wl, world):
+    """The reference's parallel-Adam CPU optimiser on the host cores,
+    bounded windows of the same workload (one window per step)."""
+    import torch
+    seed = args.seed
+    have_gpu = torch.cuda.is_available()
+    prob = make_problem(wl, seed, device_knn=have_gpu, reference_graph=True)
+    from oracle import oracle as O
+    adj = prob["adj"]
+    stt, csr = O.csr_from_graph(wl["n"], adj.ptr, adj.col, adj.w)
+    prob["A_e"] = active_edges_per_epoch(csr["eps"], wl["n_epochs"])
+    threads = os.cpu_count() or 1
+    per_step = max(1.0, args.cpu_seconds / 2)
+    for _ in range(args.warmup):
+        cpu_windows(prob, wl, seed, per_step / 4, threads)
+    updates, samples, secs = 0.0, [], 0.0
+    for _ in range(args.steps):
+        v, s, t = cpu_windows(prob, wl, seed, per_step, threads)
+        updates += v * t
+        samples.append(s)
+        secs += t
+    value = updates / secs
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": round(secs / args.steps * 1e3, 3), "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+           "config": {"workload": f"{args.workload}: {wl['desc']}", "n_points": wl["n"]},
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                            "sample": samples[0]},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,244 @@
+/*
+ * umapcu.h -- C ABI of the B200 (sm_100a) UMAP hot path.
+ *
+ * Drop-in boundary for manifolds-rs's UMAP fuzzy-graph construction and
+ * layout optimiser. Every entry point names the reference interface it
+ * replaces (paths relative to the manifolds-rs crate root). Plain pointers
+ * and sizes only; all "host" pointers are ordinary CPU memory owned by the
+ * caller, "device" pointers are CUDA global memory owned by the caller.
+ * The library owns the device buffers it allocates internally and frees
+ * them before returning (or in the matching *_destroy call).
+ *
+ * Threading: every call is synchronous with respect to its own inputs and
+ * outputs and runs on a stream the library creates per call (or per state
+ * handle). Distinct state handles may be used from distinct threads.
+ */
+#ifndef UMAPCU_H
+#define UMAPCU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes; each maps 1:1 onto a ManifoldsError variant
+ * (src/errors.rs:7-118). */
+typedef enum umapcu_status {
+    UMAPCU_OK = 0,
+    UMAPCU_NO_DATA = 1,                /* ManifoldsError::NoData (errors.rs:78) */
+    UMAPCU_NO_GRAPH_EDGES = 2,         /* ManifoldsError::NoGraphEdges (errors.rs:82) */
+    UMAPCU_DEGENERATE_LOCAL_RADII = 3, /* ManifoldsError::DegenerateLocalRadii (errors.rs:101) */
+    UMAPCU_CUDA_ALLOC = 4,             /* ManifoldsError::CubeclUtilsError (errors.rs:54): allocation */
+    UMAPCU_CUDA_LAUNCH = 5,            /* ManifoldsError::CubeclUtilsError: launch / runtime error */
+    UMAPCU_TIMEOUT = 6,                /* a bounded device wait gave up */
+    UMAPCU_BAD_ARG = 7,                /* invalid argument (null pointer, n_dim out of range, ...) */
+    UMAPCU_NO_DEVICE = 8,              /* no CUDA device usable */
+    UMAPCU_CAPACITY = 9                /* caller-provided output capacity too small */
+} umapcu_status;
+
+/* Optimiser selection: the string keys of parse_umap_optimiser_gpu
+ * (src/training/umap_optimiser_gpu.rs:44-52). "adam_gpu" -> ADAM. SGD is the
+ * per-node-gather SGD (clipped attractive term, y += lr_e * grad). */
+enum { UMAPCU_OPT_ADAM = 0, UMAPCU_OPT_SGD = 1 };
+
+/* Negative sampler. REF_HASH reproduces gpu_hash_neg
+ * (umap_optimiser_gpu.rs:611-624) bit for bit; PHILOX is Philox4x32-10
+ * keyed on (seed), counter (CSR entry, epoch, negative/4). */
+enum { UMAPCU_NEG_REF_HASH = 0, UMAPCU_NEG_PHILOX = 1 };
+
+/* UmapOptimParams<f32> (src/training/umap_optimisers.rs:24-45). */
+typedef struct umapcu_optim_params {
+    float a, b, lr, gamma;
+    uint32_t n_epochs, neg_sample_rate;
+    float min_dist, beta1, beta2, eps;
+} umapcu_optim_params;
+
+/* UmapGraphParams<f32> (src/data/graph.rs:30-41). */
+typedef struct umapcu_graph_params {
+    float bandwidth, local_connectivity, mix_weight;
+} umapcu_graph_params;
+
+/* DensState<f32> (src/utils/density.rs:140-160) with its DensParams
+ * (density.rs:69-79). r and mu_sum are host arrays of length n. */
+typedef struct umapcu_dens {
+    float lambda, frac, var_shift;
+    const float *r;
+    const float *mu_sum;
+    float mu_tot;
+} umapcu_dens;
+
+/* Human-readable name of a status code. */
+const char *umapcu_status_string(umapcu_status s);
+
+/* Library version string ("umapcu <major>.<minor>.<patch> sm_100a"). */
+const char *umapcu_version(void);
+
+/* ---------------------------------------------------------------------
+ * Parameters (host)
+ * ------------------------------------------------------------------- */
+
+/* Replaces UmapOptimParams::fit_params
+ * (src/training/umap_optimisers.rs:139-209), f32 instantiation; fits the
+ * a, b of 1/(1 + a x^2b) to min_dist/spread on the host. */
+umapcu_status umapcu_fit_ab(float min_dist, float spread, float *a, float *b);
+
+/* ---------------------------------------------------------------------
+ * Fuzzy simplicial set (graph construction), host buffers
+ * ------------------------------------------------------------------- */
+
+/* Replaces smooth_knn_dist (src/data/graph.rs:499-565). knn_dist is
+ * [n * k] row-major (self excluded, ascending per row). Writes sigma[n],
+ * rho[n]. */
+umapcu_status umapcu_smooth_knn_dist(const float *knn_dist, uint32_t n, uint32_t k,
+                                     float local_connectivity, float bandwidth, uint32_t n_iter,
+                                     float *sigma, float *rho);
+
+/* Replaces the graph stage of construct_umap_graph / construct_umap_graph_gpu
+ * (src/lib.rs:296-306, :3421-3431): smooth_knn_dist -> knn_to_coo
+ * (graph.rs:585-662) -> symmetrise_graph (graph.rs:684-694, via
+ * symmetrise_csr :387-468) -> filter_weak_edges (graph.rs:776-853).
+ * Output COO (row, col, val), grouped by row, columns ascending, nnz
+ * entries; capacity must be >= 2 * n * k (returns UMAPCU_CAPACITY
+ * otherwise). sigma/rho may be NULL. */
+umapcu_status umapcu_construct_umap_graph(const int32_t *knn_idx, const float *knn_dist, uint32_t n,
+                                          uint32_t k, const umapcu_graph_params *params,
+                                          uint32_t n_epochs, uint64_t capacity, uint32_t *row,
+                                          uint32_t *col, float *val, uint64_t *nnz, float *sigma,
+                                          float *rho);
+
+/* Replaces DensState::new (src/utils/density.rs:181-201): the constant
+ * densMAP state from the symmetrised COO and the kNN lists. Writes
+ * r[n], mu_sum[n], *mu_tot. Returns UMAPCU_DEGENERATE_LOCAL_RADII like the
+ * reference. */
+umapcu_status umapcu_dens_state_new(uint32_t n, uint64_t nnz, const uint32_t *row,
+                                    const uint32_t *col, const float *val, const int32_t *knn_idx,
+                                    const float *knn_dist, uint32_t k, int distances_squared,
+                                    float *r, float *mu_sum, float *mu_tot);
+
+/* ---------------------------------------------------------------------
+ * Layout optimiser, host buffers (the "adam_gpu" slot)
+ * ------------------------------------------------------------------- */
+
+/* Replaces optimise_embedding_adam_gpu
+ * (src/training/umap_optimiser_gpu.rs:1302-1369). embd is [n * n_dim]
+ * row-major, optimised in place. The graph is the adjacency list
+ * graph[i] = [(adj_col[p], adj_w[p]) for p in adj_ptr[i]..adj_ptr[i+1]]
+ * (the reference's Vec<Vec<(usize, T)>>); only i < j entries are used.
+ * dens may be NULL (plain UMAP). n_dim in 1..8. */
+umapcu_status umapcu_optimise_embedding(float *embd, uint32_t n, uint32_t n_dim,
+                                        const uint64_t *adj_ptr, const uint32_t *adj_col,
+                                        const float *adj_w, const umapcu_optim_params *params,
+                                        const umapcu_dens *dens, uint64_t seed, uint32_t optimiser,
+                                        uint32_t sampler, int verbose);
+
+/* ---------------------------------------------------------------------
+ * Device-resident optimiser state (UmapGpuState, umap_optimiser_gpu.rs:
+ * 278-453): upload once, run epochs, read back. Used for parity tests of
+ * single epochs and by callers that keep the state on the GPU.
+ * ------------------------------------------------------------------- */
+
+typedef struct umapcu_state umapcu_state;
+
+/* Replaces UmapCsrGraph::from_graph + UmapGpuState::upload
+ * (umap_optimiser_gpu.rs:132-209, :374-452). Builds the CSR on the device.
+ * Returns NO_DATA / NO_GRAPH_EDGES like the reference. */
+umapcu_status umapcu_state_create(const float *embd, uint32_t n, uint32_t n_dim,
+                                  const uint64_t *adj_ptr, const uint32_t *adj_col,
+                                  const float *adj_w, const umapcu_optim_params *params,
+                                  const umapcu_dens *dens, uint64_t seed, uint32_t sampler,
+                                  umapcu_state **out);
+
+void umapcu_state_destroy(umapcu_state *st);
+
+/* Number of nodes / unique undirected edges / CSR entries of the state. */
+umapcu_status umapcu_state_sizes(const umapcu_state *st, uint64_t *n, uint64_t *n_edges);
+
+/* Reads back the device CSR (offsets[n+1], edge_idx[2E], other[2E],
+ * eps[E], mu[E]); any pointer may be NULL. Same layout as UmapCsrGraph. */
+umapcu_status umapcu_state_read_csr(const umapcu_state *st, uint32_t *offsets, uint32_t *edge_idx,
+                                    uint32_t *other, float *eps, float *mu);
+
+/* Runs epochs [first, first + count) of the loop at
+ * umap_optimiser_gpu.rs:1336-1360 (densMAP update when active -> gradient
+ * -> Adam/SGD step -> schedule advance). */
+umapcu_status umapcu_state_run(umapcu_state *st, uint32_t first_epoch, uint32_t count,
+                               uint32_t optimiser);
+
+/* One epoch with inspection hooks, for parity tests (mirrors
+ * launch_grad_accum + launch_adam_update + launch_edge_schedule_update,
+ * umap_optimiser_gpu.rs:1016-1227). injected: NULL or host [2E * neg_rate]
+ * negative node per (CSR entry, negative). grad/has_update: NULL or host
+ * [n * n_dim] / [n] outputs of the gradient pass. */
+umapcu_status umapcu_state_epoch_debug(umapcu_state *st, uint32_t epoch, uint32_t optimiser,
+                                       const uint32_t *injected, float *grad, uint32_t *has_update);
+
+/* Reads the embedding / Adam moments [n * n_dim] and the per-edge
+ * schedule cursors [E]; any pointer may be NULL. */
+umapcu_status umapcu_state_read(const umapcu_state *st, float *embd, float *m, float *v,
+                                float *cursor);
+
+/* Restarts the run: embedding := embd (host [n * n_dim], NULL keeps the
+ * current one), Adam moments := 0, schedule cursors := periods
+ * (UmapGpuState::upload initial state, umap_optimiser_gpu.rs:410-441). */
+umapcu_status umapcu_state_reset(umapcu_state *st, const float *embd);
+
+/* x^b in the layout kernels: 0 (default) = 2^(b log2 x) on the MUFU units
+ * (about 1e-6 relative error), 1 = CUDA's powf. */
+umapcu_status umapcu_state_set_precise_pow(umapcu_state *st, int precise);
+
+/* Launches the state's kernels on the caller's CUDA stream (a cudaStream_t
+ * passed as void*); NULL restores the state's own stream. The caller must
+ * order its own work on that stream. */
+umapcu_status umapcu_state_set_stream(umapcu_state *st, void *cuda_stream);
+
+/* umapcu_state_run with CUDA events around every launch: *epoch_ms is the
+ * summed duration of the fused epoch kernels, *dens_ms of the densMAP
+ * updates (either may be NULL). */
+umapcu_status umapcu_state_run_profiled(umapcu_state *st, uint32_t first_epoch, uint32_t count,
+                                        uint32_t optimiser, float *epoch_ms, float *dens_ms);
+
+/* Overwrites embedding / moments ([n * n_dim], any may be NULL). */
+umapcu_status umapcu_state_write(umapcu_state *st, const float *embd, const float *m,
+                                 const float *v);
+
+/* densMAP per-epoch state after the last density update (umap_dens_radii +
+ * umap_dens_weights, umap_optimiser_gpu.rs:487-586, :1089-1143): re[n],
+ * phi_sum[n], weight[n], *coeff, and the f32 statistics (mean, std, cov).
+ * Forces a density update from the current embedding first. */
+umapcu_status umapcu_state_dens_update(umapcu_state *st, float *re, float *phi_sum, float *weight,
+                                       float *coeff, float *stats3);
+
+/* ---------------------------------------------------------------------
+ * Kernel-level test hooks (host buffers), each the reference launcher it
+ * names, run through the same device functions as the fused epoch kernel.
+ * ------------------------------------------------------------------- */
+
+/* umap_adam_update + launch_adam_update (umap_optimiser_gpu.rs:887-923,
+ * :1155-1196): in place on m, v, embd ([n * n_dim]). */
+umapcu_status umapcu_adam_update(const float *grad, const uint32_t *has_update, float *m, float *v,
+                                 float *embd, uint32_t n, uint32_t n_dim,
+                                 const umapcu_optim_params *params, uint32_t epoch);
+
+/* umap_edge_schedule_update (umap_optimiser_gpu.rs:940-955): in place on
+ * cursor[n_edges]. */
+umapcu_status umapcu_edge_schedule_update(const float *eps, float *cursor, uint64_t n_edges,
+                                          uint32_t epoch);
+
+/* x^b as the layout kernels evaluate it (F::powf in umap_grad_accum and
+ * umap_dens_radii, umap_optimiser_gpu.rs:528, :754, :832), for x > 0:
+ * out[i] = x[i]^b; precise selects CUDA's powf. */
+umapcu_status umapcu_eval_pow(const float *x, uint32_t n, float b, int precise, float *out);
+
+/* gpu_hash_neg (umap_optimiser_gpu.rs:611-624) and the Philox sampler,
+ * evaluated on the device for count consecutive neg indices. */
+umapcu_status umapcu_sample_negatives(uint32_t sampler, uint64_t seed, uint32_t node,
+                                      uint32_t entry, uint32_t epoch, uint32_t edge_local,
+                                      uint32_t count, uint32_t n, uint32_t *out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* UMAPCU_H */

@@ -1,0 +1,148 @@
+// Shared internals of the umapcu CUDA library (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdio>
+#include <cstring>
+#include <stdexcept>
+#include <vector>
+
+#include "umapcu.h"
+
+namespace umapcu {
+
+// Internal error carrier: thrown inside the library, caught at the C ABI.
+struct Error {
+    umapcu_status status;
+    const char *what;
+};
+
+[[noreturn]] inline void fail(umapcu_status s, const char *what) { throw Error{s, what}; }
+
+inline void check_cuda(cudaError_t e, const char *what, umapcu_status kind = UMAPCU_CUDA_LAUNCH)
+{
+    if (e != cudaSuccess) {
+        if (e == cudaErrorMemoryAllocation) kind = UMAPCU_CUDA_ALLOC;
+        if (getenv("UMAPCU_DEBUG"))
+            fprintf(stderr, "umapcu: %s failed: %s\n", what, cudaGetErrorString(e));
+        cudaGetLastError();
+        fail(kind, what);
+    }
+}
+
+#define UMAPCU_CK(x) ::umapcu::check_cuda((x), #x)
+
+// Stream-ordered device buffer (cudaMallocAsync / cudaFreeAsync).
+template <typename T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    cudaStream_t s = nullptr;
+    DevBuf() = default;
+    DevBuf(size_t count, cudaStream_t stream) { alloc(count, stream); }
+    void alloc(size_t count, cudaStream_t stream)
+    {
+        release();
+        s = stream;
+        n = count;
+        if (count) check_cuda(cudaMallocAsync((void **)&p, count * sizeof(T), stream), "cudaMallocAsync",
+                              UMAPCU_CUDA_ALLOC);
+    }
+    void release()
+    {
+        if (p) cudaFreeAsync(p, s);
+        p = nullptr;
+        n = 0;
+    }
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    DevBuf(DevBuf &&o) noexcept : p(o.p), n(o.n), s(o.s) { o.p = nullptr; o.n = 0; }
+    DevBuf &operator=(DevBuf &&o) noexcept
+    {
+        if (this != &o) { release(); p = o.p; n = o.n; s = o.s; o.p = nullptr; o.n = 0; }
+        return *this;
+    }
+    ~DevBuf() { release(); }
+    size_t bytes() const { return n * sizeof(T); }
+};
+
+// RAII stream owned by one API call / state.
+struct Stream {
+    cudaStream_t s = nullptr;
+    Stream() { check_cuda(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate"); }
+    ~Stream()
+    {
+        if (s) { cudaStreamSynchronize(s); cudaStreamDestroy(s); }
+    }
+    Stream(const Stream &) = delete;
+    Stream &operator=(const Stream &) = delete;
+};
+
+template <typename T>
+inline void h2d(T *dst, const T *src, size_t count, cudaStream_t s)
+{
+    if (count) check_cuda(cudaMemcpyAsync(dst, src, count * sizeof(T), cudaMemcpyHostToDevice, s), "h2d");
+}
+template <typename T>
+inline void d2h(T *dst, const T *src, size_t count, cudaStream_t s)
+{
+    if (count) check_cuda(cudaMemcpyAsync(dst, src, count * sizeof(T), cudaMemcpyDeviceToHost, s), "d2h");
+}
+inline void sync(cudaStream_t s) { check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize"); }
+inline void check_launch(const char *what) { check_cuda(cudaGetLastError(), what); }
+
+inline unsigned ceil_div(uint64_t a, uint64_t b) { return (unsigned)((a + b - 1) / b); }
+
+int device_sm_count();
+
+// ------------------------------------------------------------------ graph
+
+struct DeviceCoo {
+    DevBuf<uint32_t> row, col;
+    DevBuf<float> val;
+    uint64_t nnz = 0;
+};
+
+// smooth_knn_dist on device buffers (graph.rs:499-565).
+void smooth_knn_dist_dev(const float *d_dist, uint32_t n, uint32_t k, float local_connectivity,
+                         float bandwidth, uint32_t n_iter, float *d_sigma, float *d_rho, cudaStream_t s);
+
+// The full graph stage (lib.rs:296-306) on device buffers; the kNN arrays
+// stay owned by the caller.
+void construct_graph_dev(const int32_t *d_idx, const float *d_dist, uint32_t n, uint32_t k,
+                         const umapcu_graph_params &gp, uint32_t n_epochs, DeviceCoo &out,
+                         float *d_sigma, float *d_rho, cudaStream_t s);
+
+// densMAP constant state (density.rs:181-201) on device buffers.
+umapcu_status dens_state_dev(uint32_t n, uint64_t nnz, const uint32_t *d_row, const uint32_t *d_col,
+                             const float *d_val, const int32_t *d_idx, const float *d_dist, uint32_t k,
+                             int distances_squared, float *d_r, float *d_mu_sum, float *h_mu_tot,
+                             cudaStream_t s);
+
+// Optimiser CSR (UmapCsrGraph::from_graph, umap_optimiser_gpu.rs:132-209),
+// stored per CSR entry: other node, edge id, (cursor, period) schedule,
+// edge weight.
+struct DeviceCsr {
+    uint32_t n = 0;
+    uint64_t n_edges = 0;
+    DevBuf<uint32_t> offsets;   // [n + 1]
+    DevBuf<uint32_t> other;     // [2E + 8] (8 padding entries)
+    DevBuf<uint32_t> edge_id;   // [2E]
+    DevBuf<float2> sched;       // [2E + 8] (cursor, period); 8 padding entries for 16-byte copies
+    DevBuf<float> mu_entry;     // [2E] edge weight per entry (densMAP)
+    DevBuf<float> eps;          // [E] period per edge
+    DevBuf<float> mu;           // [E] weight per edge
+};
+
+// Builds the optimiser CSR from a device adjacency (adj_ptr [n+1], u64).
+// Returns NO_DATA / NO_GRAPH_EDGES / OK.
+umapcu_status build_csr_dev(uint32_t n, const uint64_t *d_adj_ptr, const uint32_t *d_adj_col,
+                            const float *d_adj_w, uint64_t nnz, DeviceCsr &csr, cudaStream_t s);
+
+// Resets every entry's schedule cursor to its period (upload state,
+// umap_optimiser_gpu.rs:425-430).
+void reset_schedule_dev(DeviceCsr &csr, cudaStream_t s);
+
+}  // namespace umapcu

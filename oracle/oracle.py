@@ -97,7 +97,7 @@ def lib():
                                                  C.c_float, C.c_float, C.c_float, C.c_float, C.c_uint32,
                                                  C.c_uint32, C.c_float, C.c_float, C.c_float, vp, C.c_float,
                                                  C.c_float, C.c_float, C.c_float, C.c_uint64, C.c_int,
-                                                 C.c_uint32]
+                                                 C.c_uint32, C.c_uint32, C.POINTER(C.c_double)]
         L.orc_optimise_sequential.restype = C.c_int
         L.orc_optimise_sequential.argtypes = [C.c_int, f32p, C.c_uint32, C.c_uint32, u64p, u32p, f32p,
                                               C.c_float, C.c_float, C.c_float, C.c_float, C.c_uint32,
@@ -324,16 +324,19 @@ def optimise_adam_gpu(embd, n, adj_ptr, adj_col, adj_w, p, seed, dens=None, samp
 
 
 def optimise_adam_parallel(embd, n, adj_ptr, adj_col, adj_w, p, seed, dens=None, n_threads=0,
-                           epochs_to_run=0):
-    """umap_optimisers.rs:1170-1492 (the timed CPU baseline)."""
+                           epochs_to_run=0, first_epoch=0, return_seconds=False):
+    """umap_optimisers.rs:1170-1492 (the timed CPU baseline). Runs epochs
+    [first_epoch, first_epoch + epochs_to_run) after fast-forwarding the
+    schedule; return_seconds adds the epoch loop's wall time."""
     e = np.array(embd, dtype=np.float32, order="C")
     rp, lam, frac, vs, mt, keep = _dens_args(dens)
+    secs = C.c_double(0.0)
     st = lib().orc_optimise_adam_parallel(e, n, e.shape[1], np.ascontiguousarray(adj_ptr, np.uint64),
                                           _u32(adj_col), _f32(adj_w), p["a"], p["b"], p["lr"],
                                           p["gamma"], p["n_epochs"], p["neg_sample_rate"], p["beta1"],
                                           p["beta2"], p["eps"], rp, lam, frac, vs, mt, seed, n_threads,
-                                          epochs_to_run)
-    return st, e
+                                          first_epoch, epochs_to_run, C.byref(secs))
+    return (st, e, secs.value) if return_seconds else (st, e)
 
 
 def optimise_sequential(algo, embd, n, adj_ptr, adj_col, adj_w, p, seed, dens=None):
