@@ -57,21 +57,6 @@ umapcu_status guard(F &&f)
     }
 }
 
-// launch_adam_update host scalars (umap_optimiser_gpu.rs:1164-1175)
-void epoch_scalars(const umapcu_optim_params &p, uint32_t epoch, float *fused, float *epsc, float *lr_e)
-{
-    const float one = 1.0f;
-    float lr_alpha = p.lr * (one - (float)epoch / (float)p.n_epochs);
-    float t = (float)(epoch + 1);
-    float beta1t = powf(p.beta1, t);
-    float beta2t = powf(p.beta2, t);
-    float sqrt_b2t1 = sqrtf(one - beta2t);
-    float ad_scale = sqrt_b2t1 / (one - beta1t);
-    *epsc = sqrt_b2t1 * p.eps;
-    *fused = lr_alpha * ad_scale;
-    *lr_e = lr_alpha;
-}
-
 // DensState::is_active (density.rs:244-250), T = f32
 bool dens_active(float lambda, float frac, uint32_t epoch, uint32_t n_epochs)
 {

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <stdexcept>
@@ -96,6 +97,23 @@ inline void check_launch(const char *what) { check_cuda(cudaGetLastError(), what
 inline unsigned ceil_div(uint64_t a, uint64_t b) { return (unsigned)((a + b - 1) / b); }
 
 int device_sm_count();
+
+// launch_adam_update host scalars (umap_optimiser_gpu.rs:1164-1175), f32:
+// fused = lr * (1 - e/N) * ad_scale, epsc = sqrt(1 - beta2^t) * eps, and the
+// plain learning-rate schedule lr * (1 - e/N).
+inline void epoch_scalars(const umapcu_optim_params &p, uint32_t epoch, float *fused, float *epsc, float *lr_e)
+{
+    const float one = 1.0f;
+    float lr_alpha = p.lr * (one - (float)epoch / (float)p.n_epochs);
+    float t = (float)(epoch + 1);
+    float beta1t = powf(p.beta1, t);
+    float beta2t = powf(p.beta2, t);
+    float sqrt_b2t1 = sqrtf(one - beta2t);
+    float ad_scale = sqrt_b2t1 / (one - beta1t);
+    *epsc = sqrt_b2t1 * p.eps;
+    *fused = lr_alpha * ad_scale;
+    *lr_e = lr_alpha;
+}
 
 // ------------------------------------------------------------------ graph
 
