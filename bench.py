@@ -25,7 +25,6 @@ from __future__ import annotations
 import argparse
 import json
 import os
-import subprocess
 import sys
 import threading
 import time
@@ -107,58 +106,59 @@ def active_edges_per_epoch(eps, n_epochs):
 # ----------------------------------------------------------------- clocks
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
-
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """SM clock and clock-event (throttle) reasons sampled through NVML every
+    50 ms during the timed region (reads only; no setting is changed)."""
 
     def __init__(self, device_index):
         self.dev = device_index
-        self.proc = None
-        self.lines = []
+        self.samples = []
+        self.stop = threading.Event()
+        self.t = None
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
-                 "-i", str(self.dev)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
+            import pynvml as N
+            N.nvmlInit()
+            self.N = N
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+            idx = int(vis.split(",")[self.dev]) if vis and vis.split(",")[self.dev].isdigit() else self.dev
+            self.h = N.nvmlDeviceGetHandleByIndex(idx)
+            self.max_mhz = N.nvmlDeviceGetMaxClockInfo(self.h, N.NVML_CLOCK_SM)
+            self.t = threading.Thread(target=self._run, daemon=True)
             self.t.start()
-        except (OSError, ValueError):
-            self.proc = None
+        except Exception as e:  # NVML missing: record why
+            self.err = str(e)
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def _run(self):
+        N = self.N
+        while not self.stop.is_set():
+            try:
+                mhz = N.nvmlDeviceGetClockInfo(self.h, N.NVML_CLOCK_SM)
+                rs = N.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                util = N.nvmlDeviceGetUtilizationRates(self.h).gpu
+                self.samples.append((mhz, rs, util))
+            except Exception:
+                pass
+            self.stop.wait(0.05)
 
     def __exit__(self, *exc):
-        if self.proc:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
+        self.stop.set()
+        if self.t:
+            self.t.join(timeout=2)
 
     def summary(self):
-        sm, mx, reasons = [], 0.0, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                mx = max(mx, float(f[2]))
-            except ValueError:
-                continue
-            for nm, v in zip(names, f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(nm)
-        if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled: " + getattr(self, "err", "no samples")]}
+        N = self.N
+        names = {"hw_slowdown": N.nvmlClocksEventReasonHwSlowdown,
+                 "hw_thermal_slowdown": N.nvmlClocksEventReasonHwThermalSlowdown,
+                 "sw_thermal_slowdown": N.nvmlClocksEventReasonSwThermalSlowdown,
+                 "sw_power_cap": N.nvmlClocksEventReasonSwPowerCap}
+        busy = [s for s in self.samples if s[2] > 0] or self.samples
+        reasons = sorted({k for _, rs, _ in busy for k, bit in names.items() if rs & bit})
+        return {"sm_mhz": float(np.median([s[0] for s in busy])), "sm_max_mhz": float(self.max_mhz),
+                "reasons": reasons, "samples": len(busy)}
 
 
 # ----------------------------------------------------------------- CPU leg
@@ -203,7 +203,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=8.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--profile-only", action="store_true", help="small run for ncu captures")
+    ap.add_argument("--profile-only", action="store_true", help="40 epochs only, for ncu captures")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -241,8 +241,9 @@ def main():
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > L2
 
     if args.profile_only:
+        # a short run for ncu captures: 40 epochs (capture e.g. launch 31)
         st.reset(prob["init"])
-        st.run(0, min(n_ep, 8))
+        st.run(0, min(n_ep, 40))
         torch.cuda.synchronize()
         log("[bench] profile-only run done")
         return

@@ -9,6 +9,7 @@
 #include <cfloat>
 #include <cmath>
 #include <cstdlib>
+#include <chrono>
 #include <memory>
 
 #include "internal.cuh"
@@ -135,6 +136,38 @@ void run_epoch(umapcu_state *st, uint32_t epoch, uint32_t optimiser, const uint3
     st->cur ^= 1;
 }
 
+// Optional phase timing of the host-buffer entry points (UMAPCU_TIMING=1):
+// synchronises at each mark and prints the elapsed wall time to stderr.
+struct PhaseTimer {
+    bool on = getenv("UMAPCU_TIMING") != nullptr;
+    std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+    void mark(const char *what, cudaStream_t s)
+    {
+        if (!on) return;
+        sync(s);
+        auto t1 = std::chrono::steady_clock::now();
+        fprintf(stderr, "umapcu timing: %-18s %9.3f ms\n", what,
+                std::chrono::duration<double, std::milli>(t1 - t0).count());
+        t0 = t1;
+    }
+};
+
+// Keep freed stream-ordered allocations cached in the device's default pool
+// across calls (the default release threshold of 0 returns them to the
+// driver at every synchronisation). Process-local; set once per device.
+void keep_pool_memory()
+{
+    static bool done[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64 || done[dev]) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t thr = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    done[dev] = true;
+}
+
 umapcu_status create_state(const float *embd, uint32_t n, uint32_t n_dim, const uint64_t *adj_ptr,
                            const uint32_t *adj_col, const float *adj_w, const umapcu_optim_params *params,
                            const umapcu_dens *dens, uint64_t seed, uint32_t sampler,
@@ -147,9 +180,11 @@ umapcu_status create_state(const float *embd, uint32_t n, uint32_t n_dim, const 
     const uint64_t nnz = adj_ptr[n];
     if (nnz && (!adj_col || !adj_w)) return UMAPCU_BAD_ARG;
     if (dens && (!dens->r)) return UMAPCU_BAD_ARG;
+    keep_pool_memory();
     auto st = std::make_unique<umapcu_state>();
     st->stream.s = st->own.s;
     cudaStream_t s = st->stream.s;
+    PhaseTimer T;
     st->n = n;
     st->n_dim = n_dim;
     st->p = *params;
@@ -162,8 +197,10 @@ umapcu_status create_state(const float *embd, uint32_t n, uint32_t n_dim, const 
         h2d(dptr.p, adj_ptr, n + 1, s);
         h2d(dcol.p, adj_col, nnz, s);
         h2d(dw.p, adj_w, nnz, s);
+        T.mark("graph H2D", s);
         umapcu_status rc = build_csr_dev(n, dptr.p, dcol.p, dw.p, nnz, st->csr, s);
         if (rc != UMAPCU_OK) return rc;
+        T.mark("CSR build", s);
     }
     const uint64_t nt = (uint64_t)n * n_dim;
     st->y[0].alloc(nt, s);
@@ -191,6 +228,7 @@ umapcu_status create_state(const float *embd, uint32_t n, uint32_t n_dim, const 
         check_cuda(cudaMemsetAsync(st->stats.p, 0, 8 * sizeof(float), s), "memset stats");
     }
     sync(s);
+    T.mark("state upload", s);
     out = std::move(st);
     return UMAPCU_OK;
 }
@@ -593,6 +631,7 @@ umapcu_status umapcu_optimise_embedding(float *embd, uint32_t n, uint32_t n_dim,
             printf("Running %u epochs with GPU-accelerated %s optimisation.\n", params->n_epochs,
                    optimiser == UMAPCU_OPT_SGD ? "SGD" : "Adam");
         const uint64_t nt = (uint64_t)n * n_dim;
+        PhaseTimer T;
         for (uint32_t e = 0; e < params->n_epochs; e++) {
             const bool log_now = verbose && ((e + 1) % 100 == 0 || e + 1 == params->n_epochs);
             if (!log_now) {
@@ -608,8 +647,10 @@ umapcu_status umapcu_optimise_embedding(float *embd, uint32_t n, uint32_t n_dim,
             for (float x : hg) ss += (double)x * x;
             printf(" Epoch %u / %u: grad norm %.2f\n", e + 1, params->n_epochs, sqrt(ss));
         }
+        T.mark("epochs", st->stream.s);
         d2h(embd, st->y[st->cur].p, nt, st->stream.s);
         sync(st->stream.s);
+        T.mark("embedding D2H", st->stream.s);
         return UMAPCU_OK;
     });
 }

@@ -53,6 +53,21 @@ def variable_density_mixture(n, dim, n_clusters, seed, sd_lo=0.2, sd_hi=3.0, mea
     return X.astype(np.float32), lab.astype(np.int32)
 
 
+def subspace_mixture(n, dim, n_clusters, seed, sub_dim=3, mean_sd=6.0, sd=1.0, noise=0.05):
+    """Clusters that live in random sub_dim-dimensional subspaces of the dim-D
+    space (plus small isotropic noise): data with low intrinsic dimension,
+    whose neighbourhoods a 2-D layout can preserve."""
+    rng = np.random.default_rng(seed)
+    means = rng.normal(0.0, mean_sd, (n_clusters, dim))
+    lab = rng.integers(0, n_clusters, n)
+    X = means[lab] + rng.normal(0.0, noise, (n, dim))
+    for c in range(n_clusters):
+        idx = np.nonzero(lab == c)[0]
+        q, _ = np.linalg.qr(rng.normal(size=(dim, sub_dim)))
+        X[idx] += rng.normal(0.0, sd, (idx.size, sub_dim)) @ q.T
+    return X.astype(np.float32), lab.astype(np.int32)
+
+
 def _finish(i_idx, d2, k):
     """Drop self (or the farthest if self is absent), sort ascending."""
     n = i_idx.shape[0]

@@ -7,16 +7,19 @@ from oracle import oracle as O
 
 
 @functools.lru_cache(maxsize=8)
-def knn_problem(n=3000, dim=50, k=15, clusters=10, seed=0):
+def knn_problem(n=3000, dim=50, k=15, clusters=10, seed=0, kind="isotropic"):
     import umapcu.synth as S
-    X, lab = S.isotropic_mixture(n, dim, clusters, seed)
+    if kind == "subspace":
+        X, lab = S.subspace_mixture(n, dim, clusters, seed)
+    else:
+        X, lab = S.isotropic_mixture(n, dim, clusters, seed)
     idx, dist = S.exact_knn_cpu(X, k)
     return X, lab, idx, dist
 
 
 @functools.lru_cache(maxsize=8)
-def oracle_graph(n=3000, dim=50, k=15, clusters=10, seed=0, n_epochs=200):
-    X, lab, idx, dist = knn_problem(n, dim, k, clusters, seed)
+def oracle_graph(n=3000, dim=50, k=15, clusters=10, seed=0, n_epochs=200, kind="isotropic"):
+    X, lab, idx, dist = knn_problem(n, dim, k, clusters, seed, kind)
     (r, c, v), sig, rho = O.construct_umap_graph(idx, dist, n_epochs)
     ptr = O.coo_to_adj_ptr(n, r)
     return dict(X=X, lab=lab, idx=idx, dist=dist, row=r, col=c, val=v, ptr=ptr, sigma=sig, rho=rho)
