@@ -210,6 +210,47 @@ umapcu_status umapcu_state_write(umapcu_state *st, const float *embd, const floa
 umapcu_status umapcu_state_dens_update(umapcu_state *st, float *re, float *phi_sum, float *weight,
                                        float *coeff, float *stats3);
 
+/* ---------------------------------------------------------------------
+ * Batched form: many independent layouts of uneven size advanced together
+ * (no counterpart in the reference, which optimises one embedding per call
+ * of optimise_embedding_adam_gpu, umap_optimiser_gpu.rs:1302-1369). Each
+ * problem gives the arguments of one umapcu_optimise_embedding call; all
+ * share n_dim (2..4) and n_epochs. Results equal the single-problem path's
+ * for the same (embedding, graph, params, seed).
+ * ------------------------------------------------------------------- */
+
+typedef struct umapcu_batch umapcu_batch;
+
+/* Uploads every problem and builds its CSR on the device. Arrays of
+ * n_problems pointers / values; params and seeds per problem. */
+umapcu_status umapcu_batch_create(uint32_t n_problems, const uint32_t *n, uint32_t n_dim,
+                                  const float *const *embd, const uint64_t *const *adj_ptr,
+                                  const uint32_t *const *adj_col, const float *const *adj_w,
+                                  const umapcu_optim_params *params, const uint64_t *seeds,
+                                  uint32_t sampler, umapcu_batch **out);
+
+void umapcu_batch_destroy(umapcu_batch *b);
+
+/* Times the candidate launch configurations (persistent kernel with 4/6/8
+ * CTAs per SM or one launch per epoch; scan super-chunk of 4 or 8 x 32
+ * entries) on this batch for a few epochs and keeps the fastest. */
+umapcu_status umapcu_batch_autotune(umapcu_batch *b, uint32_t *mode, uint32_t *ctas_per_sm, uint32_t *ku);
+
+/* Runs all epochs of every problem from its initial state (one CUDA graph:
+ * reset + the persistent launch, mode 1, or one launch per epoch, mode 2;
+ * mode 0 = the autotuned configuration). *ms = device time of the run.
+ * Returns UMAPCU_TIMEOUT if a bounded device wait gave up. */
+umapcu_status umapcu_batch_run(umapcu_batch *b, uint32_t mode, float *ms);
+
+/* Final embedding [n * n_dim] of one problem after umapcu_batch_run. */
+umapcu_status umapcu_batch_read(const umapcu_batch *b, uint32_t problem, float *embd);
+
+/* Failure-detection check of the persistent kernel's bounded waits: runs
+ * the batch with the epoch barrier of one problem made unsatisfiable and a
+ * wait limit of wait_limit polls; returns the status the kernel reported
+ * (UMAPCU_TIMEOUT when the bound works). The batch must be rerun after. */
+umapcu_status umapcu_batch_wait_check(umapcu_batch *b, uint32_t poisoned_problem, uint32_t wait_limit);
+
 /* Layout optimisation that allocates no device memory. No counterpart in
  * the reference: for callers that cannot allocate device memory when they
  * need a layout (inside a stream callback or host function node, under a

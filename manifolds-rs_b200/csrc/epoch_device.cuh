@@ -1,0 +1,450 @@
+// Device code of one layout epoch, shared by the single-problem kernel
+// (layout.cu) and the multi-problem kernels (batch.cu). See layout.cu for the
+// design of the warp-segment epoch.
+#pragma once
+
+#include <cfloat>
+
+#include "internal.cuh"
+#include "layout.cuh"
+
+namespace umapcu {
+
+constexpr int kWarps = 4;
+// CSR entries are scanned in super-chunks of KU x 32 entries (default kU);
+// the queue of active entries holds one super-chunk plus the carried partial
+// batch.
+constexpr int kU = 8;
+// Negatives per chunk: exactly NR when the kernel is specialised on the
+// negative sample rate (NR > 0), else 4 (one Philox block = 4 draws).
+template <int NR>
+constexpr int neg_chunk() { return NR > 0 ? NR : 4; }
+constexpr unsigned kFull = 0xFFFFFFFFu;
+
+// ------------------------------------------------------------ samplers
+
+// umap_optimiser_gpu.rs:611-624 gpu_hash_neg, with h % n evaluated by
+// Lemire's exact fastmod (Lemire, Kaser & Kurz 2019): M = 2^64 / n + 1.
+__device__ __forceinline__ uint32_t hash_neg_raw(uint32_t seed, uint32_t node, uint32_t epoch,
+                                                 uint32_t edge_local, uint32_t neg)
+{
+    uint32_t h = seed ^ (node * 0x9E3779B1u) ^ (epoch * 0x85EBCA77u) ^ (edge_local * 0xC2B2AE3Du) ^
+                 (neg * 0x27D4EB2Fu);
+    h ^= h >> 16;
+    h *= 0x7FEB352Du;
+    h ^= h >> 15;
+    h *= 0x846CA68Bu;
+    h ^= h >> 16;
+    return h;
+}
+
+__device__ __forceinline__ uint32_t fastmod_u32(uint32_t a, uint64_t M, uint32_t d)
+{
+    uint64_t lowbits = M * a;
+    return (uint32_t)__umul64hi(lowbits, d);
+}
+
+// Philox4x32-10 (Salmon, Moraes, Dror & Shaw, SC'11).
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint32_t k0, uint32_t k1)
+{
+#pragma unroll
+    for (int r = 0; r < 10; r++) {
+        uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+        uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+        c = make_uint4(hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0);
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    return c;
+}
+
+__device__ __forceinline__ uint32_t range32(uint32_t x, uint32_t n) { return __umulhi(x, n); }
+
+// ------------------------------------------------------------ helpers
+
+// L2 residency: the embedding (gathered at random every epoch) is loaded
+// with an evict_last policy; the CSR arrays (streamed once per epoch) with
+// the streaming (evict-first) qualifier, so they do not push the embedding
+// out of L2.
+__device__ __forceinline__ uint64_t l2_keep_policy()
+{
+    uint64_t pol;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+
+// COH = true: loads of data that other SMs rewrite while the kernel runs
+// (the persistent multi-problem kernel: the embedding buffers, moments and
+// cursors change roles every epoch). They go through L2 (ld.global.cg)
+// instead of the non-coherent read-only path / L1.
+template <int D, bool COH = false>
+__device__ __forceinline__ void load_row_keep(const float *__restrict__ y, uint32_t i, float (&out)[D], uint64_t pol)
+{
+    if constexpr (D == 2) {
+        const float *a = y + 2ull * i;
+        if constexpr (COH)
+            asm volatile("ld.global.cg.L2::cache_hint.v2.f32 {%0, %1}, [%2], %3;"
+                         : "=f"(out[0]), "=f"(out[1])
+                         : "l"(a), "l"(pol));
+        else
+            asm volatile("ld.global.nc.L2::cache_hint.v2.f32 {%0, %1}, [%2], %3;"
+                         : "=f"(out[0]), "=f"(out[1])
+                         : "l"(a), "l"(pol));
+    } else if constexpr (D == 4) {
+        const float *a = y + 4ull * i;
+        if constexpr (COH)
+            asm volatile("ld.global.cg.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+                         : "=f"(out[0]), "=f"(out[1]), "=f"(out[2]), "=f"(out[3])
+                         : "l"(a), "l"(pol));
+        else
+            asm volatile("ld.global.nc.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+                         : "=f"(out[0]), "=f"(out[1]), "=f"(out[2]), "=f"(out[3])
+                         : "l"(a), "l"(pol));
+    } else {
+#pragma unroll
+        for (int d = 0; d < D; d++) {
+            const float *a = y + (uint64_t)i * D + d;
+            if constexpr (COH)
+                asm volatile("ld.global.cg.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(out[d]) : "l"(a), "l"(pol));
+            else
+                asm volatile("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(out[d]) : "l"(a), "l"(pol));
+        }
+    }
+}
+
+template <int D, bool COH = false>
+__device__ __forceinline__ void load_row(const float *__restrict__ y, uint32_t i, float (&out)[D])
+{
+    if constexpr (D == 2) {
+        const float2 *a = reinterpret_cast<const float2 *>(y) + i;
+        float2 v = COH ? __ldcg(a) : __ldg(a);
+        out[0] = v.x;
+        out[1] = v.y;
+    } else if constexpr (D == 4) {
+        const float4 *a = reinterpret_cast<const float4 *>(y) + i;
+        float4 v = COH ? __ldcg(a) : __ldg(a);
+        out[0] = v.x; out[1] = v.y; out[2] = v.z; out[3] = v.w;
+    } else {
+#pragma unroll
+        for (int d = 0; d < D; d++) out[d] = COH ? __ldcg(y + (uint64_t)i * D + d) : __ldg(y + (uint64_t)i * D + d);
+    }
+}
+
+template <int D>
+__device__ __forceinline__ void store_row(float *__restrict__ y, uint32_t i, const float (&v)[D])
+{
+    if constexpr (D == 2) {
+        reinterpret_cast<float2 *>(y)[i] = make_float2(v[0], v[1]);
+    } else if constexpr (D == 4) {
+        reinterpret_cast<float4 *>(y)[i] = make_float4(v[0], v[1], v[2], v[3]);
+    } else {
+#pragma unroll
+        for (int d = 0; d < D; d++) y[(uint64_t)i * D + d] = v[d];
+    }
+}
+
+// x^b for the strictly positive x of the UMAP kernels (dist_sq >= 1e-8,
+// dist_sq + 0.001): 2^(b * log2 x) on the MUFU units (lg2.approx /
+// ex2.approx, no subnormal inputs occur). Relative error about 1e-6 over
+// x in [1e-8, 1e6] against the correctly rounded power (checked on the device
+// by the test suite), a few ulp; CUDA's full-range powf costs ~30x the
+// instructions. `precise` selects CUDA's powf instead.
+__device__ __forceinline__ float pow_pos(float x, float b, bool precise)
+{
+    if (precise) return powf(x, b);
+    float l, r;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(l) : "f"(x));
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(b * l));
+    return r;
+}
+
+// a / b for the kernels' positive denominators (>= 1e-11): IEEE division
+// when `precise`, else a * rcp.approx(b) (2 ulp).
+__device__ __forceinline__ float div_k(float a, float b, bool precise)
+{
+    return precise ? a / b : __fdividef(a, b);
+}
+
+__device__ __forceinline__ float clip4(float x)
+{
+    if (x > 4.0f) x = 4.0f;
+    if (x < -4.0f) x = -4.0f;
+    return x;
+}
+
+// umap_adam_update (umap_optimiser_gpu.rs:912-922) for one coordinate.
+__device__ __forceinline__ float adam_coord(float g, float &m, float &v, float y, float fused, float epsc,
+                                           float omb1, float omb2)
+{
+    float m_new = m + omb1 * (g - m);
+    m = m_new;
+    float v_new = v + omb2 * (g * g - v);
+    v = v_new;
+    return y + fused * m_new / (sqrtf(v_new) + epsc);
+}
+
+// densMAP per-node weight (umap_dens_weights, umap_optimiser_gpu.rs:584-585).
+__device__ __forceinline__ float dens_weight(float r, float re, const float *__restrict__ st)
+{
+    // st = {mean, std, cov, inv_var, coeff}
+    return r - st[2] * (re - st[0]) * st[3];
+}
+
+template <int D, int KU = kU>
+struct WarpSmem {
+    static constexpr int kQ = 32 * KU + 32;
+    uint32_t beg[33];
+    uint32_t qp[kQ];
+    uint32_t qo[kQ];
+    uint8_t qj[kQ];
+    uint8_t run_len[32];
+    uint8_t run_start[32];
+    float ys[32][D];
+    float part[32][D];
+    float4 dn[32];
+};
+
+__device__ __forceinline__ uint32_t local_node(const uint32_t *beg, uint32_t p)
+{
+    // largest j in [0, 31] with beg[j] <= p
+    uint32_t j = 0;
+#pragma unroll
+    for (uint32_t step = 16; step > 0; step >>= 1)
+        if (beg[j + step] <= p) j += step;
+    return j;
+}
+
+// One batch of `cnt` queued active entries (cnt <= 32) starting at queue
+// slot q0; lane t = slot q0 + t.
+template <int D, bool DENS, int NR, bool COH, int KU>
+__device__ __forceinline__ void process_batch(const EpochArgs &A, WarpSmem<D, KU> &S, uint32_t q0, uint32_t cnt,
+                                              uint32_t node0, int lane, float (&g)[D], bool &act,
+                                              const float *dstat)
+{
+    const bool live = (uint32_t)lane < cnt;
+    uint32_t j = 0;
+    if (live) {
+        const uint32_t p = S.qp[q0 + lane], o = S.qo[q0 + lane];
+        j = S.qj[q0 + lane];
+        const uint32_t self = node0 + j;
+        float ys[D], yo[D], c[D];
+#pragma unroll
+        for (int d = 0; d < D; d++) { ys[d] = S.ys[j][d]; c[d] = 0.0f; }
+        const uint64_t pol = l2_keep_policy();
+        load_row_keep<D, COH>(A.y_cur, o, yo, pol);
+        float4 dno;
+        float mu_e = 1.0f;
+        if constexpr (DENS) {
+            dno = __ldg(A.dens_node + o);
+            mu_e = __ldg(A.mu_entry + p);
+        }
+        // attractive (umap_optimiser_gpu.rs:746-762)
+        float dist_sq = 0.0f;
+#pragma unroll
+        for (int d = 0; d < D; d++) {
+            float diff = ys[d] - yo[d];
+            dist_sq += diff * diff;
+        }
+        if (dist_sq >= 1e-8f) {
+            float dist_sq_b = pow_pos(dist_sq, A.b, A.precise_pow);
+            float denom = 1.0f + A.a * dist_sq_b;
+            float grad_coeff = div_k(A.two_a_b * dist_sq_b, dist_sq * denom, A.precise_pow);
+            if (A.optimiser == UMAPCU_OPT_SGD) {
+#pragma unroll
+                for (int d = 0; d < D; d++) c[d] += 2.0f * clip4(grad_coeff * (yo[d] - ys[d]));
+            } else {
+#pragma unroll
+                for (int d = 0; d < D; d++) c[d] += 2.0f * grad_coeff * (yo[d] - ys[d]);
+            }
+            if constexpr (DENS) {
+                // umap_optimiser_gpu.rs:769-798
+                const float4 dns = S.dn[j];
+                float phi = 1.0f / denom;
+                float dphi_term = A.a * A.b * dist_sq_b / dist_sq * phi;
+                float common = 1.0f - A.b * (1.0f - phi);
+                float dr_self = (phi / dns.x) * (common / dns.y + dphi_term);
+                float dr_other = (phi / dno.x) * (common / dno.y + dphi_term);
+                float w_s = dens_weight(dns.z, dns.w, dstat), w_o = dens_weight(dno.z, dno.w, dstat);
+                float cor = dstat[4] * (w_s * dr_self + w_o * dr_other) / mu_e;
+                float two_cor = 2.0f * cor;
+#pragma unroll
+                for (int d = 0; d < D; d++) c[d] += 2.0f * clip4(two_cor * (ys[d] - yo[d]));
+            }
+        }
+        // negatives (umap_optimiser_gpu.rs:801-849), gathered in chunks
+        const uint32_t edge_local = p - S.beg[j];
+        constexpr int kNegChunk = neg_chunk<NR>();
+        const uint32_t neg_rate = NR > 0 ? (uint32_t)NR : A.neg_rate;
+        for (uint32_t k0 = 0; k0 < neg_rate; k0 += kNegChunk) {
+            uint32_t kk[kNegChunk];
+            float yk[kNegChunk][D];
+            uint4 ph = make_uint4(0, 0, 0, 0);
+#pragma unroll
+            for (int t = 0; t < kNegChunk; t++) {
+                const uint32_t neg = k0 + t;
+                uint32_t kn = self;
+                if (neg < neg_rate) {
+                    if (A.injected) {
+                        kn = A.injected[(uint64_t)p * neg_rate + neg];
+                    } else if (A.sampler == UMAPCU_NEG_PHILOX) {
+                        if ((t & 3) == 0) ph = philox4x32_10(make_uint4(p, A.epoch, neg >> 2, 0x554D4150u), A.seed_lo,
+                                                             A.seed_hi);
+                        uint32_t r = (t & 3) == 0 ? ph.x : (t & 3) == 1 ? ph.y : (t & 3) == 2 ? ph.z : ph.w;
+                        kn = range32(r, A.n);
+                    } else {
+                        kn = fastmod_u32(hash_neg_raw(A.seed32, self, A.epoch, edge_local, neg), A.fastmod_M, A.n);
+                    }
+                }
+                kk[t] = kn;
+                if (neg < neg_rate) load_row_keep<D, COH>(A.y_cur, kn, yk[t], pol);
+            }
+#pragma unroll
+            for (int t = 0; t < kNegChunk; t++) {
+                if (k0 + t < neg_rate && kk[t] != self) {
+                    float dsk = 0.0f;
+#pragma unroll
+                    for (int d = 0; d < D; d++) {
+                        float diff = ys[d] - yk[t][d];
+                        dsk += diff * diff;
+                    }
+                    float dist_sq_safe = dsk + 0.001f;
+                    float dist_sq_b = pow_pos(dist_sq_safe, A.b, A.precise_pow);
+                    float denom = dist_sq_safe * (1.0f + A.a * dist_sq_b);
+                    float gc = clip4(div_k(A.two_gamma_b, denom, A.precise_pow));
+#pragma unroll
+                    for (int d = 0; d < D; d++) c[d] += gc * (ys[d] - yk[t][d]);
+                }
+            }
+        }
+#pragma unroll
+        for (int d = 0; d < D; d++) S.part[lane][d] = c[d];
+    }
+    // run of slots per node (slots are sorted by local node)
+    S.run_len[lane] = 0;
+    __syncwarp();
+    const unsigned live_mask = __ballot_sync(kFull, live);
+    if (live) {
+        unsigned same = __match_any_sync(live_mask, j);
+        if (lane == __ffs(same) - 1) {
+            S.run_start[j] = (uint8_t)lane;
+            S.run_len[j] = (uint8_t)__popc(same);
+        }
+    }
+    __syncwarp();
+    const uint32_t len = S.run_len[lane];
+    if (len) {
+        act = true;
+        const uint32_t s0 = S.run_start[lane];
+        for (uint32_t s = s0; s < s0 + len; s++) {
+#pragma unroll
+            for (int d = 0; d < D; d++) g[d] += S.part[s][d];
+        }
+    }
+    __syncwarp();
+}
+
+// One epoch of one 32-node segment [node0, node0 + 32) of problem A, run by
+// one warp (see the file comment).
+template <int D, bool DENS, int NR, bool COH, int KU = kU>
+__device__ __forceinline__ void epoch_segment(const EpochArgs &A, WarpSmem<D, KU> &S, uint32_t node0, int lane)
+{
+    __syncwarp();  // the warp's shared memory may still be read by its previous segment
+    const uint32_t node = node0 + lane;
+    const bool valid = node < A.n;
+    S.beg[lane] = A.offsets[valid ? node : A.n];
+    if (lane == 31) S.beg[32] = A.offsets[min(node0 + 32u, A.n)];
+    float ys[D];
+    if (valid) load_row<D, COH>(A.y_cur, node, ys);
+    else {
+#pragma unroll
+        for (int d = 0; d < D; d++) ys[d] = 0.0f;
+    }
+#pragma unroll
+    for (int d = 0; d < D; d++) S.ys[lane][d] = ys[d];
+    const float *dstat = A.dens_stats;
+    if constexpr (DENS) {
+        if (valid) S.dn[lane] = __ldg(A.dens_node + node);
+    }
+    // Degenerate self beyond the last beg (beg[32] read by the search only
+    // through j + step <= 31 + 1).
+    float g[D];
+#pragma unroll
+    for (int d = 0; d < D; d++) g[d] = 0.0f;
+    bool act = false;
+    __syncwarp();
+    const uint32_t seg_beg = S.beg[0], seg_end = S.beg[32];
+    const unsigned lt_mask = (1u << lane) - 1u;
+    uint32_t count = 0;
+    float *cursor = reinterpret_cast<float *>(A.sched);
+    // Scan in super-chunks of kU x 32 entries: all loads of a super-chunk are
+    // issued before the first is used.
+    for (uint32_t c0 = seg_beg; c0 < seg_end; c0 += 32u * KU) {
+        float2 sv[KU];
+        uint32_t ov[KU];
+#pragma unroll
+        for (int u = 0; u < KU; u++) {
+            const uint32_t p = c0 + 32u * u + lane;
+            sv[u] = make_float2(__int_as_float(0x7f800000), 0.0f);
+            ov[u] = 0;
+            if (p < seg_end) {
+                sv[u] = COH ? __ldcg(A.sched + p) : __ldcs(A.sched + p);
+                ov[u] = __ldcs(A.other + p);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < KU; u++) {
+            const uint32_t p = c0 + 32u * u + lane;
+            const bool a = sv[u].x <= A.epoch_f;  // out-of-range lanes hold +inf
+            if (a) __stcs(cursor + 2 * (uint64_t)p, sv[u].x + sv[u].y);  // umap_edge_schedule_update
+            const unsigned mask = __ballot_sync(kFull, a);
+            if (a) {
+                const uint32_t slot = count + __popc(mask & lt_mask);
+                S.qp[slot] = p;
+                S.qo[slot] = ov[u];
+                S.qj[slot] = (uint8_t)local_node(S.beg, p);
+            }
+            count += __popc(mask);
+        }
+        __syncwarp();
+        const bool more = c0 + 32u * KU < seg_end;
+        // every full batch, and at the end of the segment the remainder too
+        const bool last = !more;
+        const uint32_t upto = last ? count : (count & ~31u);
+        for (uint32_t q0 = 0; q0 < upto; q0 += 32)
+            process_batch<D, DENS, NR, COH, KU>(A, S, q0, min(32u, upto - q0), node0, lane, g, act, dstat);
+        const uint32_t rem = count - upto;
+        if (upto && rem) {
+            uint32_t tp = 0, to = 0;
+            uint8_t tj = 0;
+            if ((uint32_t)lane < rem) { tp = S.qp[upto + lane]; to = S.qo[upto + lane]; tj = S.qj[upto + lane]; }
+            __syncwarp();
+            if ((uint32_t)lane < rem) { S.qp[lane] = tp; S.qo[lane] = to; S.qj[lane] = tj; }
+            __syncwarp();
+        }
+        count = rem;
+    }
+    if (!valid) return;
+    float yn[D];
+    if (act) {
+        if (A.optimiser == UMAPCU_OPT_SGD) {
+#pragma unroll
+            for (int d = 0; d < D; d++) yn[d] = ys[d] + A.lr_sgd * g[d];
+        } else {
+            float m[D], v[D];
+            load_row<D, COH>(A.m, node, m);
+            load_row<D, COH>(A.v, node, v);
+#pragma unroll
+            for (int d = 0; d < D; d++) yn[d] = adam_coord(g[d], m[d], v[d], ys[d], A.fused, A.epsc, A.omb1, A.omb2);
+            store_row<D>(A.m, node, m);
+            store_row<D>(A.v, node, v);
+        }
+    } else {
+#pragma unroll
+        for (int d = 0; d < D; d++) yn[d] = ys[d];
+    }
+    store_row<D>(A.y_next, node, yn);
+    if (A.dbg_grad) store_row<D>(A.dbg_grad, node, g);
+    if (A.dbg_active) A.dbg_active[node] = act ? 1u : 0u;
+}
+
+}  // namespace umapcu

@@ -126,6 +126,11 @@ _SIGS = {
     "umapcu_state_set_stream": [_vp, _vp],
     "umapcu_state_run_profiled": [_vp, _u32, _u32, _u32, _vp, _vp],
     "umapcu_state_set_precise_pow": [_vp, _i32],
+    "umapcu_batch_create": [_u32, _vp, _u32, _vp, _vp, _vp, _vp, _vp, _vp, _u32, _vp],
+    "umapcu_batch_autotune": [_vp, _vp, _vp, _vp],
+    "umapcu_batch_run": [_vp, _u32, _vp],
+    "umapcu_batch_read": [_vp, _u32, _vp],
+    "umapcu_batch_wait_check": [_vp, _u32, _u32],
     "umapcu_eval_pow": [_vp, _u32, _f32, _i32, _vp],
 }
 for _name, _args in _SIGS.items():
@@ -134,6 +139,8 @@ for _name, _args in _SIGS.items():
     _fn.restype = _i32
 _lib.umapcu_state_destroy.argtypes = [_vp]
 _lib.umapcu_state_destroy.restype = None
+_lib.umapcu_batch_destroy.argtypes = [_vp]
+_lib.umapcu_batch_destroy.restype = None
 
 
 def lib():
@@ -456,6 +463,67 @@ class UmapGpuState:
         st = np.empty(3, np.float32)
         _check(_lib.umapcu_state_dens_update(self._h, _p(re), _p(phi), _p(w), C.byref(coeff), _p(st)))
         return dict(re=re, phi_sum=phi, weight=w, coeff=np.float32(coeff.value), stats=st)
+
+
+class UmapBatch:
+    """Batched form: many independent layouts of uneven size advanced together
+    by one persistent launch (captured in a CUDA graph), configuration picked
+    by the library's autotuner. Each problem is one
+    optimise_embedding_adam_gpu call's worth of arguments; the results equal
+    the single-problem path's."""
+
+    def __init__(self, embds, graphs, params, seeds, sampler: int = NEG_REF_HASH):
+        P = len(embds)
+        if not (len(graphs) == P and len(seeds) == P):
+            raise ManifoldsError(BAD_ARG, "embds, graphs and seeds must have one entry per problem")
+        plist = params if isinstance(params, (list, tuple)) else [params] * P
+        self._e = [_c(e, np.float32) for e in embds]
+        self._a = [_adj(g) for g in graphs]
+        self.n = [e.shape[0] for e in self._e]
+        self.n_dim = self._e[0].shape[1] if P else 2
+        self.params = plist
+        arr = lambda xs, dt: (C.c_void_p * P)(*[x.ctypes.data for x in xs])
+        self._ptrs = [_c(a.ptr, np.uint64) for a in self._a]
+        cp = (_OptimParams * P)(*[q._c() for q in plist])
+        ns = np.array(self.n, np.uint32)
+        sd = np.array([int(x) & (2 ** 64 - 1) for x in seeds], np.uint64)
+        self._h = C.c_void_p()
+        _check(_lib.umapcu_batch_create(P, _p(ns), self.n_dim, arr(self._e, None), arr(self._ptrs, None),
+                                        arr([a.col for a in self._a], None), arr([a.w for a in self._a], None),
+                                        C.cast(cp, C.c_void_p), _p(sd), sampler, C.byref(self._h)))
+
+    def autotune(self):
+        m, c, k = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        _check(_lib.umapcu_batch_autotune(self._h, C.byref(m), C.byref(c), C.byref(k)))
+        return dict(mode=m.value, ctas_per_sm=c.value, ku=k.value)
+
+    def run(self, mode: int = 0) -> float:
+        """All epochs of every problem; returns device milliseconds.
+        mode 0 = autotuned, 1 = persistent launch, 2 = one launch per epoch."""
+        ms = C.c_float()
+        _check(_lib.umapcu_batch_run(self._h, mode, C.byref(ms)))
+        return ms.value
+
+    def read(self, p: int) -> np.ndarray:
+        out = np.empty((self.n[p], self.n_dim), np.float32)
+        _check(_lib.umapcu_batch_read(self._h, p, _p(out)))
+        return out
+
+    def wait_check(self, poisoned_problem: int, wait_limit: int) -> int:
+        """Status of a run whose persistent-kernel barrier for one problem can
+        never open (the bounded wait must report UMAPCU_TIMEOUT)."""
+        return _lib.umapcu_batch_wait_check(self._h, poisoned_problem, wait_limit)
+
+    def close(self):
+        if self._h:
+            _lib.umapcu_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def optimise_embedding_adam_gpu(embd: np.ndarray, graph, params: UmapOptimParams, dens: Optional[DensState] = None,
