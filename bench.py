@@ -45,6 +45,17 @@ WORKLOADS = {
                     "weights), exact kNN k=15 cached, 2-D, 200 epochs, Adam, neg_rate 5, random U(-10,10) init"),
     "c1": dict(n=10_000, dim=50, clusters=10, k=15, n_epochs=500, kind="isotropic", dens=False,
                desc="10k x 50 f32, 10 isotropic Gaussians, exact kNN k=15, 2-D, 500 epochs, Adam, neg_rate 5"),
+    "c4": dict(n=0, problems=512, n_lo=500, n_hi=50_000, dim=30, clusters=(5, 15), k=15, n_epochs=200,
+               kind="batch", dens=False,
+               desc="batched form: 512 independent problems, n log-uniform in [500, 50000], 30-D isotropic "
+                    "5-15-cluster mixtures, exact kNN k=15, 2-D, 200 epochs, Adam, one persistent launch "
+                    "(CUDA graph), configuration from the autotuner"),
+    "c5": dict(n=0, requests=2000, pool=48, n_lo=1000, n_hi=200_000, dims=(20, 50, 100), clusters=(5, 40), k=15,
+               n_epochs=200, kind="serve", dens=False, budget=120 << 30, util=0.8,
+               desc="served form: 2000 requests, seeded Poisson arrivals at ~80% of measured capacity, sizes "
+                    "log-uniform in [1000, 200000], data dims in {20, 50, 100}, 5-40 clusters, precomputed k=15 "
+                    "graphs (a pool of 48, requests draw a graph and their own seed/init), 2-D, 200 epochs, Adam, "
+                    "120 GB admission budget, continuous batching"),
     "c3": dict(n=200_000, dim=30, clusters=20, k=30, n_epochs=200, kind="variable", dens=True,
                desc="densMAP 200k x 30 f32, 20 clusters sd log-U[0.2,3], k=30, 2-D, 200 epochs, last 30% "
                     "density term, lambda 2, Adam"),
@@ -204,6 +215,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--profile-only", action="store_true", help="40 epochs only, for ncu captures")
+    ap.add_argument("--requests", type=int, default=0, help="served workload: number of requests")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -216,6 +228,12 @@ def main():
         if rank != 0:
             return
         run_reference(args, wl, world)
+        return
+    if wl["kind"] == "batch":
+        run_batched(args, wl, world, rank, local_rank)
+        return
+    if wl["kind"] == "serve":
+        run_served(args, wl, world, rank, local_rank)
         return
 
     torch.cuda.set_device(local_rank)
@@ -366,6 +384,170 @@ def main():
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def make_batch_problems(wl, seed):
+    """The C4 problem set: seeded sizes, data, exact kNN, CUDA graph stage."""
+    import umapcu
+    import umapcu.synth as S
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(wl["n_lo"]), np.log(wl["n_hi"]), wl["problems"])).astype(int)
+    adjs, inits = [], []
+    t0 = time.time()
+    for i, n in enumerate(sizes):
+        X, _ = S.isotropic_mixture(int(n), wl["dim"], int(rng.integers(wl["clusters"][0], wl["clusters"][1] + 1)),
+                                   seed + 1000 + i)
+        idx, dist = S.exact_knn_torch(X, wl["k"])
+        g = umapcu.construct_umap_graph(idx, dist, umapcu.UmapGraphParams(), wl["n_epochs"])
+        adjs.append(umapcu.coo_to_adjacency_list(g))
+        inits.append(umapcu.random_layout(int(n), 2, seed + 5000 + i))
+    log(f"[bench] {len(sizes)} problems, {int(sizes.sum())} points, prepared in {time.time() - t0:.1f}s")
+    return sizes, adjs, inits
+
+
+def run_batched(args, wl, world, rank, local_rank):
+    """Batched form vs sequential single-problem runs, embeddings/s."""
+    import torch
+    import umapcu
+    torch.cuda.set_device(local_rank)
+    seed = args.seed + rank
+    sizes, adjs, inits = make_batch_problems(wl, seed)
+    params = umapcu.UmapOptimParams.from_min_dist_spread(0.1, 1.0, n_epochs=wl["n_epochs"], neg_sample_rate=5)
+    seeds = [seed + i for i in range(len(sizes))]
+    B = umapcu.UmapBatch(inits, adjs, params, seeds)
+    cfg = B.autotune()
+    for _ in range(args.warmup):
+        B.run(0)
+    with ClockSampler(local_rank) as clk:
+        ms = [B.run(0) for _ in range(args.steps)]
+    t_batch = float(np.sum(ms)) / 1e3
+    # edge-updates per run, from each problem's periods
+    updates = 0
+    states = []
+    for i in range(len(sizes)):
+        st = umapcu.UmapGpuState(inits[i], adjs[i], params, None, seeds[i])
+        updates += int(active_edges_per_epoch(st.csr()["eps"], wl["n_epochs"]).sum())
+        states.append(st)
+    # sequential plain-kernel runs of the same problems (device-resident states)
+    stream = torch.cuda.current_stream()
+    for st in states:
+        st.set_stream(stream.cuda_stream)
+    for i, st in enumerate(states[:8]):
+        st.reset(inits[i])
+        st.run(0, wl["n_epochs"])
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for i, st in enumerate(states):
+        st.reset(inits[i])
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for st in states:
+        st.run(0, wl["n_epochs"])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_seq = e0.elapsed_time(e1) / 1e3
+    # identical results in the batch and alone (spot check)
+    ok = True
+    for i in (0, len(sizes) // 2, len(sizes) - 1):
+        y_single, _, _, _ = states[i].read()
+        ok &= bool(np.array_equal(B.read(i), y_single))
+    for st in states:
+        st.close()
+    P = len(sizes)
+    value = world * args.steps * P / t_batch
+    out = {"metric": "UMAP batched embeddings/s (512 problems)", "value": value, "unit": "embeddings/s",
+           "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": round(t_batch / args.steps * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+           "config": {"workload": f"c4: {wl['desc']}", "problems": P, "points": int(sizes.sum()),
+                      "autotuned": cfg, "l2": "not flushed (state reset kernel precedes every run)"},
+           "edge_updates_per_s": world * args.steps * updates / t_batch,
+           "sequential_plain": {"embeddings_per_s": P / t_seq, "ms": round(t_seq * 1e3, 3)},
+           "speedup_vs_sequential": round((P / t_batch * args.steps) / (P / t_seq), 2) if t_seq > 0 else None,
+           "same_result_alone_and_batched": ok,
+           "gpu_launches": args.steps * 2,
+           "clocks": clk.summary()}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    B.close()
+
+
+def run_served(args, wl, world, rank, local_rank):
+    """Continuous-batching server under a Poisson request stream."""
+    import torch
+    import umapcu
+    import umapcu.synth as S
+    torch.cuda.set_device(local_rank)
+    seed = args.seed + rank
+    rng = np.random.default_rng(seed)
+    t0 = time.time()
+    pool = []
+    for i in range(wl["pool"]):
+        n = int(np.exp(rng.uniform(np.log(wl["n_lo"]), np.log(wl["n_hi"]))))
+        dim = int(rng.choice(wl["dims"]))
+        X, _ = S.isotropic_mixture(n, dim, int(rng.integers(wl["clusters"][0], wl["clusters"][1] + 1)), seed + 70 + i)
+        idx, dist = S.exact_knn_torch(X, wl["k"])
+        g = umapcu.construct_umap_graph(idx, dist, umapcu.UmapGraphParams(), wl["n_epochs"])
+        pool.append(umapcu.coo_to_adjacency_list(g))
+    log(f"[bench] served pool of {len(pool)} graphs prepared in {time.time() - t0:.1f}s")
+    params = umapcu.UmapOptimParams.from_min_dist_spread(0.1, 1.0, n_epochs=wl["n_epochs"], neg_sample_rate=5)
+    n_req = args.requests or wl["requests"]
+    req_graph = rng.integers(0, len(pool), n_req)
+
+    def init_of(r):
+        g = int(req_graph[r])
+        return umapcu.random_layout(pool[g].n, 2, seed + 9000 + r)
+
+    # capacity: the pool as one batch, admission (copies + graph builds)
+    # included, embeddings/s for this size mix
+    b_inits = [init_of(r) for r in range(len(pool))]
+    b_graphs = [pool[int(req_graph[r])] for r in range(len(pool))]
+    umapcu.UmapBatch(b_inits, b_graphs, params, list(range(len(pool)))).close()  # warm-up
+    torch.cuda.synchronize()
+    tb = time.perf_counter()
+    B = umapcu.UmapBatch(b_inits, b_graphs, params, list(range(len(pool))))
+    t_admit = time.perf_counter() - tb
+    B.run(1)
+    t_layout = B.run(1) / 1e3
+    B.close()
+    cap = len(pool) / (t_admit + t_layout)
+    lam = wl["util"] * cap
+    gaps = rng.exponential(1.0 / lam, n_req)
+    inits = [init_of(r) for r in range(n_req)]  # client-side data, made before the stream starts
+    sv = umapcu.UmapServer(budget_bytes=wl["budget"], max_jobs=4096, tick_epochs=10, n_dim=2)
+    tickets = []
+    t_start = time.perf_counter()
+    t_next = t_start
+    with ClockSampler(local_rank) as clk:
+        for r in range(n_req):
+            t_next += gaps[r]
+            d = t_next - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            tickets.append(sv.submit(inits[r], pool[int(req_graph[r])], params, seed=seed + r))
+        t_sub = time.perf_counter()
+        lat, queue = [], []
+        for t in tickets:
+            _, l, q = sv.wait(t)
+            lat.append(l)
+            queue.append(q)
+        t_end = time.perf_counter()
+    st = sv.stats()
+    sv.close()
+    span = t_end - t_start
+    out = {"metric": "UMAP served embeddings/s (Poisson stream)", "value": n_req / span, "unit": "embeddings/s",
+           "n_gpus": world, "steps": 1, "warmup": 0, "ms_per_step": round(span * 1e3, 3),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+           "config": {"workload": f"c5: {wl['desc']}", "requests": n_req, "arrival_rate_per_s": round(lam, 2),
+                      "submitted_rate_per_s": round(n_req / (t_sub - t_start), 2),
+                      "capacity_per_s": round(cap, 2), "layout_only_capacity_per_s": round(len(pool) / t_layout, 2),
+                      "budget_bytes": wl["budget"], "tick_epochs": 10},
+           "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                         "mean": float(np.mean(lat)), "max": float(np.max(lat))},
+           "queue_s": {"p50": float(np.percentile(queue, 50)), "p99": float(np.percentile(queue, 99))},
+           "server": st, "clocks": clk.summary()}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
 
 
 def run_reference(args, wl, world):

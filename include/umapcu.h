@@ -35,7 +35,8 @@ typedef enum umapcu_status {
     UMAPCU_TIMEOUT = 6,                /* a bounded device wait gave up */
     UMAPCU_BAD_ARG = 7,                /* invalid argument (null pointer, n_dim out of range, ...) */
     UMAPCU_NO_DEVICE = 8,              /* no CUDA device usable */
-    UMAPCU_CAPACITY = 9                /* caller-provided output capacity too small */
+    UMAPCU_CAPACITY = 9,               /* output capacity / device budget / scratch too small */
+    UMAPCU_CANCELLED = 10              /* a served job was cancelled or the server shut down */
 } umapcu_status;
 
 /* Optimiser selection: the string keys of parse_umap_optimiser_gpu
@@ -250,6 +251,51 @@ umapcu_status umapcu_batch_read(const umapcu_batch *b, uint32_t problem, float *
  * wait limit of wait_limit polls; returns the status the kernel reported
  * (UMAPCU_TIMEOUT when the bound works). The batch must be rerun after. */
 umapcu_status umapcu_batch_wait_check(umapcu_batch *b, uint32_t poisoned_problem, uint32_t wait_limit);
+
+/* ---------------------------------------------------------------------
+ * Served form: continuous batching of layout jobs (no counterpart in the
+ * reference). A server thread owns the device: it admits submitted jobs in
+ * arrival order within a device-memory budget and a job-count limit, and
+ * every tick advances all admitted jobs by tick_epochs epochs -- each from
+ * its own current epoch -- in one persistent launch. Each job's result equals
+ * the single-problem path's for the same arguments, alone or in any mix.
+ * All calls are thread-safe.
+ * ------------------------------------------------------------------- */
+
+typedef struct umapcu_server umapcu_server;
+
+/* Starts a server on the current device. device_budget_bytes bounds the
+ * summed peak-memory estimate of admitted jobs; all jobs share n_dim (2..4). */
+umapcu_status umapcu_server_create(uint64_t device_budget_bytes, uint32_t max_jobs, uint32_t tick_epochs,
+                                   uint32_t n_dim, umapcu_server **out);
+
+/* Queues one job (the arguments of umapcu_optimise_embedding, copied) and
+ * returns at once with its ticket. UMAPCU_CAPACITY if the job alone exceeds
+ * the budget. */
+umapcu_status umapcu_server_submit(umapcu_server *sv, uint32_t n, uint32_t n_dim, const float *embd,
+                                   const uint64_t *adj_ptr, const uint32_t *adj_col, const float *adj_w,
+                                   const umapcu_optim_params *params, uint64_t seed, uint32_t sampler,
+                                   uint64_t *ticket);
+
+/* *state: 0 pending, 1 running, 2 done, 3 failed or cancelled. */
+umapcu_status umapcu_server_poll(umapcu_server *sv, uint64_t ticket, int *state);
+
+/* Cancels a job that has not been admitted yet (its wait returns
+ * UMAPCU_CANCELLED). */
+umapcu_status umapcu_server_cancel(umapcu_server *sv, uint64_t ticket);
+
+/* Blocks until the job finishes, copies its embedding [n * n_dim] (if
+ * embd_out is not NULL) and forgets the ticket. *latency_s = submit to
+ * completion, *queue_s = submit to admission. Returns the job's status. */
+umapcu_status umapcu_server_wait(umapcu_server *sv, uint64_t ticket, float *embd_out, double *latency_s,
+                                 double *queue_s);
+
+umapcu_status umapcu_server_stats(umapcu_server *sv, uint64_t *completed, uint64_t *ticks,
+                                  uint64_t *peak_bytes, uint32_t *peak_jobs);
+
+/* Stops the server after the current tick; unfinished jobs fail with
+ * UMAPCU_CANCELLED. */
+void umapcu_server_destroy(umapcu_server *sv);
 
 /* Layout optimisation that allocates no device memory. No counterpart in
  * the reference: for callers that cannot allocate device memory when they

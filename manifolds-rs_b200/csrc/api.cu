@@ -9,6 +9,7 @@
 #include <cfloat>
 #include <cmath>
 #include <cstdlib>
+#include <atomic>
 #include <chrono>
 #include <memory>
 
@@ -152,21 +153,6 @@ struct PhaseTimer {
     }
 };
 
-// Keep freed stream-ordered allocations cached in the device's default pool
-// across calls (the default release threshold of 0 returns them to the
-// driver at every synchronisation). Process-local; set once per device.
-void keep_pool_memory()
-{
-    static bool done[64] = {};
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64 || done[dev]) return;
-    cudaMemPool_t pool;
-    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
-        uint64_t thr = UINT64_MAX;
-        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
-    }
-    done[dev] = true;
-}
 
 umapcu_status create_state(const float *embd, uint32_t n, uint32_t n_dim, const uint64_t *adj_ptr,
                            const uint32_t *adj_col, const float *adj_w, const umapcu_optim_params *params,
@@ -256,6 +242,22 @@ __global__ void k_dens_weight_out(uint32_t n, const float4 *__restrict__ dn, con
 
 }  // namespace
 
+// Keep freed stream-ordered allocations cached in the device's default pool
+// across calls (the default release threshold of 0 returns them to the
+// driver at every synchronisation). Process-local; set once per device.
+void umapcu::keep_pool_memory()
+{
+    static std::atomic<bool> done[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64 || done[dev].load()) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t thr = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    done[dev].store(true);
+}
+
 // ------------------------------------------------------------------ ABI
 
 extern "C" {
@@ -272,7 +274,8 @@ const char *umapcu_status_string(umapcu_status s)
         case UMAPCU_TIMEOUT: return "bounded device wait timed out";
         case UMAPCU_BAD_ARG: return "bad argument";
         case UMAPCU_NO_DEVICE: return "no CUDA device";
-        case UMAPCU_CAPACITY: return "output capacity too small";
+        case UMAPCU_CAPACITY: return "capacity exceeded (output buffer, device budget or scratch)";
+        case UMAPCU_CANCELLED: return "cancelled";
     }
     return "unknown status";
 }

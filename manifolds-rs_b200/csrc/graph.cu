@@ -201,10 +201,16 @@ static int bits_for(uint64_t v)
     return b;
 }
 
-// Exclusive scan of u32 flags; returns the total.
-static uint64_t scan_flags(const uint32_t *d_flags, uint32_t *d_pos, uint64_t m, cudaStream_t s)
+// Exclusive scan of u32 flags; returns the total. d_word (optional): a
+// device word read back in the same synchronisation.
+static uint64_t scan_flags(const uint32_t *d_flags, uint32_t *d_pos, uint64_t m, cudaStream_t s,
+                           const uint32_t *d_word = nullptr, uint32_t *h_word = nullptr)
 {
-    if (!m) return 0;
+    if (d_word) d2h(h_word, d_word, 1, s);
+    if (!m) {
+        if (d_word) sync(s);
+        return 0;
+    }
     size_t tb = 0;
     check_cuda(cub::DeviceScan::ExclusiveSum(nullptr, tb, d_flags, d_pos, (int64_t)m, s), "scan size");
     DevBuf<char> tmp(tb ? tb : 1, s);
@@ -302,14 +308,19 @@ __device__ __forceinline__ uint32_t row_of(const uint64_t *__restrict__ ptr, uin
     return lo;
 }
 
+// Upper-triangle entries (i < j) become edges. A column outside [0, n) is
+// reported in *bad and its entry dropped (the reference indexes out of range).
 __global__ void k_upper_flags(const uint64_t *__restrict__ adj_ptr, const uint32_t *__restrict__ adj_col,
-                              uint32_t n, uint64_t nnz, uint32_t *__restrict__ src_row, uint32_t *__restrict__ flag)
+                              uint32_t n, uint64_t nnz, uint32_t *__restrict__ src_row, uint32_t *__restrict__ flag,
+                              uint32_t *__restrict__ bad)
 {
     uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= nnz) return;
     uint32_t i = row_of(adj_ptr, n, p);
+    const uint32_t c = adj_col[p];
     src_row[p] = i;
-    flag[p] = i < adj_col[p];
+    if (c >= n) *bad = 1u;
+    flag[p] = i < c && c < n;
 }
 
 __global__ void k_edges(const uint32_t *__restrict__ src_row, const uint32_t *__restrict__ adj_col,
@@ -327,14 +338,16 @@ __global__ void k_edges(const uint32_t *__restrict__ src_row, const uint32_t *__
 
 // umap_optimiser_gpu.rs:186-196: period = 1 / (w / max_w), 1e8 when the
 // normalised weight is not positive. Endpoint records (node, 2e + side).
+// node_job (several graphs in one build): the maximum is the edge's own
+// graph's, d_max indexed by graph.
 __global__ void k_edge_records(const uint32_t *__restrict__ ei, const uint32_t *__restrict__ ej,
                                const float *__restrict__ ew, uint64_t E, const float *__restrict__ d_max,
                                float *__restrict__ eps, uint32_t *__restrict__ key, uint32_t *__restrict__ val,
-                               uint32_t *__restrict__ degree)
+                               uint32_t *__restrict__ degree, const uint32_t *__restrict__ node_job)
 {
     uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= E) return;
-    float norm = ew[e] / *d_max;
+    float norm = ew[e] / d_max[node_job ? node_job[ei[e]] : 0];
     eps[e] = norm > 0.0f ? 1.0f / norm : 1e8f;
     key[2 * e] = ei[e];
     val[2 * e] = (uint32_t)(2 * e);
@@ -344,11 +357,14 @@ __global__ void k_edge_records(const uint32_t *__restrict__ ei, const uint32_t *
     atomicAdd(&degree[ej[e]], 1u);
 }
 
+// node_job / node_base (several graphs in one build): `other` is written as
+// an index local to its graph.
 __global__ void k_csr_entries(const uint32_t *__restrict__ val_s, uint64_t tot, const uint32_t *__restrict__ ei,
                               const uint32_t *__restrict__ ej, const float *__restrict__ ew,
                               const float *__restrict__ eps, uint32_t *__restrict__ other,
                               uint32_t *__restrict__ edge_id, float2 *__restrict__ sched,
-                              float *__restrict__ mu_entry)
+                              float *__restrict__ mu_entry, const uint32_t *__restrict__ node_job,
+                              const uint32_t *__restrict__ node_base)
 {
     uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= tot + 8) return;
@@ -360,7 +376,8 @@ __global__ void k_csr_entries(const uint32_t *__restrict__ val_s, uint64_t tot, 
     }
     uint32_t v = val_s[p];
     uint32_t e = v >> 1;
-    other[p] = (v & 1) ? ei[e] : ej[e];
+    uint32_t o = (v & 1) ? ei[e] : ej[e];
+    other[p] = node_job ? o - node_base[node_job[o]] : o;
     edge_id[p] = e;
     float pe = eps[e];
     sched[p] = make_float2(pe, pe);
@@ -389,12 +406,15 @@ umapcu_status build_csr_dev(uint32_t n, const uint64_t *d_adj_ptr, const uint32_
     if (n == 0) return UMAPCU_NO_DATA;
     if (nnz >= (1ull << 31)) fail(UMAPCU_BAD_ARG, "graph too large for 32-bit CSR entries");
     csr.n = n;
-    DevBuf<uint32_t> src_row(nnz, s), flag(nnz, s), pos(nnz, s);
+    DevBuf<uint32_t> src_row(nnz, s), flag(nnz, s), pos(nnz, s), bad(1, s);
+    check_cuda(cudaMemsetAsync(bad.p, 0, sizeof(uint32_t), s), "memset");
     if (nnz) {
-        k_upper_flags<<<ceil_div(nnz, 256), 256, 0, s>>>(d_adj_ptr, d_adj_col, n, nnz, src_row.p, flag.p);
+        k_upper_flags<<<ceil_div(nnz, 256), 256, 0, s>>>(d_adj_ptr, d_adj_col, n, nnz, src_row.p, flag.p, bad.p);
         check_launch("k_upper_flags");
     }
-    uint64_t E = scan_flags(flag.p, pos.p, nnz, s);
+    uint32_t bad_h = 0;
+    uint64_t E = scan_flags(flag.p, pos.p, nnz, s, bad.p, &bad_h);
+    if (bad_h) return UMAPCU_BAD_ARG;
     if (E == 0) return UMAPCU_NO_GRAPH_EDGES;
     csr.n_edges = E;
     DevBuf<uint32_t> ei(E, s), ej(E, s);
@@ -410,7 +430,7 @@ umapcu_status build_csr_dev(uint32_t n, const uint64_t *d_adj_ptr, const uint32_
     DevBuf<uint32_t> key(tot, s), val(tot, s), key_s(tot, s), val_s(tot, s), degree(n + 1, s);
     check_cuda(cudaMemsetAsync(degree.p, 0, sizeof(uint32_t) * (n + 1), s), "memset");
     k_edge_records<<<ceil_div(E, 256), 256, 0, s>>>(ei.p, ej.p, csr.mu.p, E, dmax.p, csr.eps.p, key.p, val.p,
-                                                    degree.p);
+                                                    degree.p, nullptr);
     check_launch("k_edge_records");
     int end_bit = bits_for(n);
     size_t tb = 0;
@@ -435,7 +455,154 @@ umapcu_status build_csr_dev(uint32_t n, const uint64_t *d_adj_ptr, const uint32_
     csr.sched.alloc(tot + 8, s);
     csr.mu_entry.alloc(tot, s);
     k_csr_entries<<<ceil_div(tot + 8, 256), 256, 0, s>>>(val_s.p, tot, ei.p, ej.p, csr.mu.p, csr.eps.p, csr.other.p,
-                                                         csr.edge_id.p, csr.sched.p, csr.mu_entry.p);
+                                                         csr.edge_id.p, csr.sched.p, csr.mu_entry.p, nullptr,
+                                                         nullptr);
+    check_launch("k_csr_entries");
+    return UMAPCU_OK;
+}
+
+// ---------------------------------------------- several graphs, one build
+
+__global__ void k_node_job(const uint32_t *__restrict__ node_base, uint32_t n_jobs, uint32_t n_total,
+                           uint32_t *__restrict__ node_job)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_total) return;
+    uint32_t lo = 0, hi = n_jobs;  // largest t with node_base[t] <= i
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (node_base[mid] <= i) lo = mid;
+        else hi = mid;
+    }
+    node_job[i] = lo;
+}
+
+// k_upper_flags over concatenated graphs: the entry's graph by its first
+// entry (job_entry_base [J + 1]), its row inside the graph's own local ptr
+// (graph t's ptr starts at lptr + node_base[t] + t), the row and column made
+// global. Columns outside the graph are reported and dropped.
+__global__ void k_upper_flags_multi(const uint64_t *__restrict__ lptr, const uint32_t *__restrict__ adj_col,
+                                    const uint32_t *__restrict__ node_base, const uint64_t *__restrict__ job_entry_base,
+                                    uint32_t n_jobs, uint64_t nnz, uint32_t *__restrict__ src_row,
+                                    uint32_t *__restrict__ gcol, uint32_t *__restrict__ flag, uint32_t *__restrict__ bad)
+{
+    uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= nnz) return;
+    uint32_t lo = 0, hi = n_jobs;  // largest t with job_entry_base[t] <= p
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (job_entry_base[mid] <= p) lo = mid;
+        else hi = mid;
+    }
+    const uint32_t nb = node_base[lo], nj = node_base[lo + 1] - nb;
+    const uint32_t il = row_of(lptr + nb + lo, nj, p - job_entry_base[lo]);
+    const uint32_t c = adj_col[p];
+    src_row[p] = nb + il;
+    gcol[p] = nb + c;
+    if (c >= nj) *bad = 1u;
+    flag[p] = il < c && c < nj;
+}
+
+// Edges per job from the exclusive scan of the upper flags.
+__global__ void k_job_edges(const uint32_t *__restrict__ flag, const uint32_t *__restrict__ pos, uint64_t nnz,
+                            const uint64_t *__restrict__ job_entry_base, uint32_t n_jobs,
+                            uint64_t *__restrict__ job_edges)
+{
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t > n_jobs) return;
+    // edges before entry a: pos[a] (a < nnz) or the total
+    const uint64_t a = job_entry_base[t];
+    job_edges[t] = a < nnz ? pos[a] : (uint64_t)pos[nnz - 1] + flag[nnz - 1];
+}
+
+// Per-job maximum weight from 0 (the single build's MaxFrom0 reduction):
+// non-negative floats order like their bit patterns, NaN never enters.
+__global__ void k_job_max(const uint32_t *__restrict__ ei, const float *__restrict__ ew, uint64_t E,
+                          const uint32_t *__restrict__ node_job, float *__restrict__ dmax)
+{
+    uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= E) return;
+    const float w = ew[e];
+    if (w > 0.0f) atomicMax((int *)&dmax[node_job[ei[e]]], __float_as_int(w));
+}
+
+umapcu_status build_csr_multi(uint32_t n_total, uint32_t n_jobs, const uint32_t *d_node_base,
+                              const uint64_t *d_job_entry_base, const uint64_t *d_lptr, const uint32_t *d_adj_col,
+                              const float *d_adj_w, uint64_t nnz, DeviceCsr &csr, uint64_t *h_job_edges,
+                              cudaStream_t s)
+{
+    if (n_total == 0 || n_jobs == 0) return UMAPCU_NO_DATA;
+    if (nnz >= (1ull << 31)) fail(UMAPCU_BAD_ARG, "graphs too large for 32-bit CSR entries");
+    if (nnz == 0) return UMAPCU_NO_GRAPH_EDGES;
+    csr.n = n_total;
+    DevBuf<uint32_t> node_job(n_total, s);
+    k_node_job<<<ceil_div(n_total, 256), 256, 0, s>>>(d_node_base, n_jobs, n_total, node_job.p);
+    check_launch("k_node_job");
+    DevBuf<uint32_t> src_row(nnz, s), gcol(nnz, s), flag(nnz, s), pos(nnz, s), bad(1, s);
+    check_cuda(cudaMemsetAsync(bad.p, 0, sizeof(uint32_t), s), "memset");
+    k_upper_flags_multi<<<ceil_div(nnz, 256), 256, 0, s>>>(d_lptr, d_adj_col, d_node_base, d_job_entry_base, n_jobs,
+                                                           nnz, src_row.p, gcol.p, flag.p, bad.p);
+    check_launch("k_upper_flags_multi");
+    {
+        size_t tb = 0;
+        check_cuda(cub::DeviceScan::ExclusiveSum(nullptr, tb, flag.p, pos.p, (int64_t)nnz, s), "scan size");
+        DevBuf<char> tmp(tb ? tb : 1, s);
+        check_cuda(cub::DeviceScan::ExclusiveSum(tmp.p, tb, flag.p, pos.p, (int64_t)nnz, s), "scan");
+    }
+    DevBuf<uint64_t> je(n_jobs + 1, s);
+    k_job_edges<<<ceil_div(n_jobs + 1, 256), 256, 0, s>>>(flag.p, pos.p, nnz, d_job_entry_base, n_jobs, je.p);
+    check_launch("k_job_edges");
+    std::vector<uint64_t> cum(n_jobs + 1);
+    uint32_t bad_h = 0;
+    d2h(cum.data(), je.p, n_jobs + 1, s);
+    d2h(&bad_h, bad.p, 1, s);
+    sync(s);
+    if (bad_h) return UMAPCU_BAD_ARG;
+    for (uint32_t t = 0; t < n_jobs; t++) h_job_edges[t] = cum[t + 1] - cum[t];
+    const uint64_t E = cum[n_jobs] - cum[0];
+    if (E == 0) return UMAPCU_NO_GRAPH_EDGES;
+    csr.n_edges = E;
+    DevBuf<uint32_t> ei(E, s), ej(E, s);
+    csr.mu.alloc(E, s);
+    k_edges<<<ceil_div(nnz, 256), 256, 0, s>>>(src_row.p, gcol.p, d_adj_w, flag.p, pos.p, nnz, ei.p, ej.p, csr.mu.p);
+    check_launch("k_edges");
+    src_row.release(); gcol.release(); flag.release(); pos.release();
+    DevBuf<float> dmax(n_jobs, s);
+    check_cuda(cudaMemsetAsync(dmax.p, 0, sizeof(float) * n_jobs, s), "memset");
+    k_job_max<<<ceil_div(E, 256), 256, 0, s>>>(ei.p, csr.mu.p, E, node_job.p, dmax.p);
+    check_launch("k_job_max");
+    const uint64_t tot = 2 * E;
+    csr.eps.alloc(E, s);
+    DevBuf<uint32_t> key(tot, s), val(tot, s), key_s(tot, s), val_s(tot, s), degree(n_total + 1, s);
+    check_cuda(cudaMemsetAsync(degree.p, 0, sizeof(uint32_t) * (n_total + 1), s), "memset");
+    k_edge_records<<<ceil_div(E, 256), 256, 0, s>>>(ei.p, ej.p, csr.mu.p, E, dmax.p, csr.eps.p, key.p, val.p,
+                                                    degree.p, node_job.p);
+    check_launch("k_edge_records");
+    const int end_bit = bits_for(n_total);
+    {
+        size_t tb = 0;
+        check_cuda(cub::DeviceRadixSort::SortPairs(nullptr, tb, key.p, key_s.p, val.p, val_s.p, (int64_t)tot, 0,
+                                                   end_bit, s), "sort size");
+        DevBuf<char> tmp(tb ? tb : 1, s);
+        check_cuda(cub::DeviceRadixSort::SortPairs(tmp.p, tb, key.p, key_s.p, val.p, val_s.p, (int64_t)tot, 0,
+                                                   end_bit, s), "sort");
+    }
+    csr.offsets.alloc(n_total + 1, s);
+    {
+        size_t tb2 = 0;
+        check_cuda(cub::DeviceScan::ExclusiveSum(nullptr, tb2, degree.p, csr.offsets.p, (int64_t)(n_total + 1), s),
+                   "scan size");
+        DevBuf<char> tmp(tb2 ? tb2 : 1, s);
+        check_cuda(cub::DeviceScan::ExclusiveSum(tmp.p, tb2, degree.p, csr.offsets.p, (int64_t)(n_total + 1), s),
+                   "scan");
+    }
+    csr.other.alloc(tot + 8, s);
+    csr.edge_id.alloc(tot, s);
+    csr.sched.alloc(tot + 8, s);
+    csr.mu_entry.alloc(tot, s);
+    k_csr_entries<<<ceil_div(tot + 8, 256), 256, 0, s>>>(val_s.p, tot, ei.p, ej.p, csr.mu.p, csr.eps.p, csr.other.p,
+                                                         csr.edge_id.p, csr.sched.p, csr.mu_entry.p, node_job.p,
+                                                         d_node_base);
     check_launch("k_csr_entries");
     return UMAPCU_OK;
 }

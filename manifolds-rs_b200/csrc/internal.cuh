@@ -73,6 +73,14 @@ struct DevBuf {
 struct Stream {
     cudaStream_t s = nullptr;
     Stream() { check_cuda(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate"); }
+    // highest = true: the device's greatest stream priority (its CTAs are
+    // dispatched ahead of default-priority work as SMs free up)
+    explicit Stream(bool highest)
+    {
+        int lo = 0, hi = 0;
+        check_cuda(cudaDeviceGetStreamPriorityRange(&lo, &hi), "cudaDeviceGetStreamPriorityRange");
+        check_cuda(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, highest ? hi : lo), "cudaStreamCreate");
+    }
     ~Stream()
     {
         if (s) { cudaStreamSynchronize(s); cudaStreamDestroy(s); }
@@ -97,6 +105,9 @@ inline void check_launch(const char *what) { check_cuda(cudaGetLastError(), what
 inline unsigned ceil_div(uint64_t a, uint64_t b) { return (unsigned)((a + b - 1) / b); }
 
 int device_sm_count();
+// Keeps freed stream-ordered allocations cached in the current device's
+// default pool (release threshold raised from 0); set once per device.
+void keep_pool_memory();
 
 // launch_adam_update host scalars (umap_optimiser_gpu.rs:1164-1175), f32:
 // fused = lr * (1 - e/N) * ad_scale, epsc = sqrt(1 - beta2^t) * eps, and the
@@ -158,6 +169,22 @@ struct DeviceCsr {
 // Returns NO_DATA / NO_GRAPH_EDGES / OK.
 umapcu_status build_csr_dev(uint32_t n, const uint64_t *d_adj_ptr, const uint32_t *d_adj_col,
                             const float *d_adj_w, uint64_t nnz, DeviceCsr &csr, cudaStream_t s);
+
+// Several graphs built as one (the served form's admission). The graphs'
+// adjacencies are concatenated: lptr holds each graph's own row pointers
+// (graph t's n_t + 1 entries start at lptr + node_base[t] + t, counting from
+// 0), adj_col / adj_w its entries from job_entry_base[t], columns local to
+// the graph; node_base [n_jobs + 1] and job_entry_base [n_jobs + 1] are the
+// graphs' first global node and first entry. The CSR spans all nodes; each
+// node's row equals the single-graph build's (same entries in the same order,
+// `other` local to the graph, periods normalised by the graph's own maximum
+// weight), so graph t's slice (offsets + node_base[t], the shared other /
+// sched arrays) is a drop-in for its own build. h_job_edges [n_jobs] receives
+// edges per graph. A column outside its graph returns BAD_ARG.
+umapcu_status build_csr_multi(uint32_t n_total, uint32_t n_jobs, const uint32_t *d_node_base,
+                              const uint64_t *d_job_entry_base, const uint64_t *d_lptr, const uint32_t *d_adj_col,
+                              const float *d_adj_w, uint64_t nnz, DeviceCsr &csr, uint64_t *h_job_edges,
+                              cudaStream_t s);
 
 // Resets every entry's schedule cursor to its period (upload state,
 // umap_optimiser_gpu.rs:425-430).

@@ -40,7 +40,7 @@ _lib = C.CDLL(LIB_PATH)
 # ------------------------------------------------------------------ errors
 
 OK, NO_DATA, NO_GRAPH_EDGES, DEGENERATE_LOCAL_RADII = 0, 1, 2, 3
-CUDA_ALLOC, CUDA_LAUNCH, TIMEOUT, BAD_ARG, NO_DEVICE, CAPACITY = 4, 5, 6, 7, 8, 9
+CUDA_ALLOC, CUDA_LAUNCH, TIMEOUT, BAD_ARG, NO_DEVICE, CAPACITY, CANCELLED = 4, 5, 6, 7, 8, 9, 10
 
 OPT_ADAM, OPT_SGD = 0, 1
 NEG_REF_HASH, NEG_PHILOX = 0, 1
@@ -72,9 +72,13 @@ class CubeclUtilsError(ManifoldsError):
     CubeclUtilsError variant (src/errors.rs:54)."""
 
 
+class Cancelled(ManifoldsError):
+    """A served job was cancelled or its server shut down."""
+
+
 _ERR = {NO_DATA: NoData, NO_GRAPH_EDGES: NoGraphEdges, DEGENERATE_LOCAL_RADII: DegenerateLocalRadii,
         CUDA_ALLOC: CubeclUtilsError, CUDA_LAUNCH: CubeclUtilsError, TIMEOUT: CubeclUtilsError,
-        NO_DEVICE: CubeclUtilsError}
+        NO_DEVICE: CubeclUtilsError, CANCELLED: Cancelled}
 
 
 def _check(st: int, what: str = ""):
@@ -131,6 +135,12 @@ _SIGS = {
     "umapcu_batch_run": [_vp, _u32, _vp],
     "umapcu_batch_read": [_vp, _u32, _vp],
     "umapcu_batch_wait_check": [_vp, _u32, _u32],
+    "umapcu_server_create": [_u64, _u32, _u32, _u32, _vp],
+    "umapcu_server_submit": [_vp, _u32, _u32, _vp, _vp, _vp, _vp, _vp, _u64, _u32, _vp],
+    "umapcu_server_poll": [_vp, _u64, _vp],
+    "umapcu_server_cancel": [_vp, _u64],
+    "umapcu_server_wait": [_vp, _u64, _vp, _vp, _vp],
+    "umapcu_server_stats": [_vp, _vp, _vp, _vp, _vp],
     "umapcu_eval_pow": [_vp, _u32, _f32, _i32, _vp],
 }
 for _name, _args in _SIGS.items():
@@ -141,6 +151,8 @@ _lib.umapcu_state_destroy.argtypes = [_vp]
 _lib.umapcu_state_destroy.restype = None
 _lib.umapcu_batch_destroy.argtypes = [_vp]
 _lib.umapcu_batch_destroy.restype = None
+_lib.umapcu_server_destroy.argtypes = [_vp]
+_lib.umapcu_server_destroy.restype = None
 
 
 def lib():
@@ -517,6 +529,66 @@ class UmapBatch:
     def close(self):
         if self._h:
             _lib.umapcu_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class UmapServer:
+    """Served form: continuous batching of layout jobs on one GPU. submit()
+    returns at once; the library's server thread admits jobs within the
+    device-memory budget and advances all admitted jobs together, each from
+    its own epoch. Thread-safe."""
+
+    PENDING, RUNNING, DONE, FAILED = 0, 1, 2, 3
+
+    def __init__(self, budget_bytes: int, max_jobs: int = 4096, tick_epochs: int = 10, n_dim: int = 2):
+        self._h = C.c_void_p()
+        self.n_dim = n_dim
+        self._n = {}
+        _check(_lib.umapcu_server_create(int(budget_bytes), max_jobs, tick_epochs, n_dim, C.byref(self._h)))
+
+    def submit(self, embd, graph, params: UmapOptimParams, seed: int = 42, sampler: int = NEG_REF_HASH) -> int:
+        e = _c(embd, np.float32)
+        a = _adj(graph)
+        cp = params._c()
+        t = C.c_uint64()
+        _check(_lib.umapcu_server_submit(self._h, e.shape[0], e.shape[1], _p(e), _p(_c(a.ptr, np.uint64)), _p(a.col),
+                                         _p(a.w), C.byref(cp), int(seed) & (2 ** 64 - 1), sampler, C.byref(t)))
+        self._n[t.value] = e.shape[0]
+        return t.value
+
+    def poll(self, ticket: int) -> int:
+        st = C.c_int()
+        _check(_lib.umapcu_server_poll(self._h, ticket, C.byref(st)))
+        return st.value
+
+    def cancel(self, ticket: int):
+        _check(_lib.umapcu_server_cancel(self._h, ticket))
+
+    def wait(self, ticket: int):
+        """-> (embedding [n, n_dim], latency_s, queue_s); raises on failure."""
+        n = self._n.pop(ticket, None)
+        if n is None:
+            raise ManifoldsError(BAD_ARG, "unknown ticket")
+        out = np.empty((n, self.n_dim), np.float32)
+        lat, q = C.c_double(), C.c_double()
+        _check(_lib.umapcu_server_wait(self._h, ticket, _p(out), C.byref(lat), C.byref(q)))
+        return out, lat.value, q.value
+
+    def stats(self):
+        c, t, b = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        j = C.c_uint32()
+        _check(_lib.umapcu_server_stats(self._h, C.byref(c), C.byref(t), C.byref(b), C.byref(j)))
+        return dict(completed=c.value, ticks=t.value, peak_bytes=b.value, peak_jobs=j.value)
+
+    def close(self):
+        if self._h:
+            _lib.umapcu_server_destroy(self._h)
             self._h = C.c_void_p()
 
     def __del__(self):

@@ -115,6 +115,10 @@ def test_errors_match_reference():
         umapcu.UmapGpuState(TRI_EMBD, [[], [], []], _tri_params())
     with pytest.raises(umapcu.NoData):
         umapcu.UmapGpuState(np.zeros((0, 2), np.float32), [], _tri_params())
+    # a neighbour index past the last node (the reference's Vec indexing
+    # panics): rejected on the device before any edge is formed
+    with pytest.raises(umapcu.ManifoldsError):
+        umapcu.UmapGpuState(TRI_EMBD, [[(1, 1.0), (3, 0.5)], [(0, 1.0)], [(0, 0.5)]], _tri_params())
 
 
 # ------------------------------------------------------------- kernels
