@@ -69,9 +69,10 @@ def log(*a):
 # ----------------------------------------------------------------- inputs
 
 def make_problem(wl, seed, device_knn=True, reference_graph=False):
-    """Synthetic data -> exact kNN (torch on the GPU: input preparation) ->
-    fuzzy graph: the CUDA graph stage for the umapcu arm, the oracle's CPU
-    restatement of the reference's graph stage for the reference arm."""
+    """Synthetic data -> exact kNN (input preparation: the library's GPU
+    kernel for the umapcu arm, torch for the reference arm) -> fuzzy graph:
+    the CUDA graph stage for the umapcu arm, the oracle's CPU restatement of
+    the reference's graph stage for the reference arm."""
     import umapcu
     import umapcu.synth as S
     t0 = time.time()
@@ -81,7 +82,10 @@ def make_problem(wl, seed, device_knn=True, reference_graph=False):
         X, _ = S.variable_density_mixture(wl["n"], wl["dim"], wl["clusters"], seed)
     else:
         X, _ = S.isotropic_mixture(wl["n"], wl["dim"], wl["clusters"], seed)
-    idx, dist = S.exact_knn_torch(X, wl["k"]) if device_knn else S.exact_knn_cpu(X, wl["k"])
+    if reference_graph:
+        idx, dist = S.exact_knn_torch(X, wl["k"]) if device_knn else S.exact_knn_cpu(X, wl["k"])
+    else:
+        idx, dist = umapcu.knn_exact(X, wl["k"])
     t1 = time.time()
     if reference_graph:
         from oracle import oracle as O
@@ -353,6 +357,15 @@ def main():
         e2e = {"value": world * e2e_steps * updates_per_step / et, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(embd_p.nbytes), "ms_per_step": round(et / e2e_steps * 1e3, 3)}
 
+    quality = None
+    if e2e is not None and rank == 0:
+        # the finished embedding of the last end-to-end run, on a seeded
+        # 10 000-query subsample against all points
+        qn = min(10_000, wl["n"])
+        qs = np.sort(np.random.default_rng(seed + 77).choice(wl["n"], qn, replace=False)).astype(np.uint32)
+        q = umapcu.embedding_quality(prob["X"], embd_p, prob["idx"], 15, queries=qs)
+        quality = {"trust15": q["trust"], "knn_preservation15": q["knn_preservation"], "queries": int(qn)}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -378,6 +391,7 @@ def main():
             "gpu_launches": args.steps * (n_ep + dens_launches),
             "clocks": clk.summary(),
             "densmap_ms_per_step": round(d_ms, 3) if wl["dens"] else None,
+            "quality": quality,
         }
         print(json.dumps(out), flush=True)
     st.close()
@@ -397,7 +411,7 @@ def make_batch_problems(wl, seed):
     for i, n in enumerate(sizes):
         X, _ = S.isotropic_mixture(int(n), wl["dim"], int(rng.integers(wl["clusters"][0], wl["clusters"][1] + 1)),
                                    seed + 1000 + i)
-        idx, dist = S.exact_knn_torch(X, wl["k"])
+        idx, dist = umapcu.knn_exact(X, wl["k"])
         g = umapcu.construct_umap_graph(idx, dist, umapcu.UmapGraphParams(), wl["n_epochs"])
         adjs.append(umapcu.coo_to_adjacency_list(g))
         inits.append(umapcu.random_layout(int(n), 2, seed + 5000 + i))
@@ -486,7 +500,7 @@ def run_served(args, wl, world, rank, local_rank):
         n = int(np.exp(rng.uniform(np.log(wl["n_lo"]), np.log(wl["n_hi"]))))
         dim = int(rng.choice(wl["dims"]))
         X, _ = S.isotropic_mixture(n, dim, int(rng.integers(wl["clusters"][0], wl["clusters"][1] + 1)), seed + 70 + i)
-        idx, dist = S.exact_knn_torch(X, wl["k"])
+        idx, dist = umapcu.knn_exact(X, wl["k"])
         g = umapcu.construct_umap_graph(idx, dist, umapcu.UmapGraphParams(), wl["n_epochs"])
         pool.append(umapcu.coo_to_adjacency_list(g))
     log(f"[bench] served pool of {len(pool)} graphs prepared in {time.time() - t0:.1f}s")

@@ -351,6 +351,61 @@ umapcu_status umapcu_sample_negatives(uint32_t sampler, uint64_t seed, uint32_t 
                                       uint32_t entry, uint32_t epoch, uint32_t edge_local,
                                       uint32_t count, uint32_t n, uint32_t *out);
 
+/* ------------------------------------------------ kNN, metrics, kNN cache */
+
+/* Distance metrics of the neighbour search (NearestNeighbourParams::
+ * dist_metric, src/data/nearest_neighbours.rs:44, "euclidean" | "cosine").
+ * Euclidean distances are returned SQUARED, as the reference's ANN backends
+ * return them (src/lib.rs:435); cosine distance is 1 - <x/|x|, y/|y|>. */
+enum { UMAPCU_METRIC_EUCLIDEAN_SQ = 0, UMAPCU_METRIC_COSINE = 1 };
+
+/* Exact k nearest neighbours of every row of x [n * dim] (host), self
+ * excluded: replaces run_ann_search with AnnSearch::Exhaustive
+ * (src/data/nearest_neighbours.rs:225-364, which queries k + 1 and drops the
+ * first) as the source of the precomputed kNN (PreComputedKnn, src/lib.rs:79).
+ * knn_idx / knn_dist [n * k] (host), ascending by distance, ties by index.
+ * Each distance is the sequential f32 FMA chain over the dimensions in order
+ * (d = fma(x_i - y_i, x_i - y_i, d)). Needs 0 < k <= 32 and n > k. */
+umapcu_status umapcu_knn_exact(const float *x, uint32_t n, uint32_t dim, uint32_t k, uint32_t metric,
+                               int32_t *knn_idx, float *knn_dist);
+
+/* The same on device buffers, for the rows d_queries [n_queries] of d_x
+ * (nullptr: every row, n_queries = n), on `stream` (cudaStream_t; nullptr =
+ * legacy default stream). d_idx / d_dist [n_queries * k]. */
+umapcu_status umapcu_knn_exact_dev(const float *d_x, uint32_t n, uint32_t dim, const uint32_t *d_queries,
+                                   uint32_t n_queries, uint32_t k, uint32_t metric, uint32_t *d_idx,
+                                   float *d_dist, void *stream);
+
+/* Embedding quality (no reference counterpart; the reference has no
+ * metrics). trust: trustworthiness@k with sklearn.manifold.trustworthiness's
+ * definition over the query rows (all rows when queries is nullptr, then
+ * equal to sklearn's value up to f32 distance rounding); knn_preservation:
+ * mean |kNN_X(i)[:k] & kNN_Y(i)| / k with kNN_X from knn_idx [n * knn_k].
+ * Either output may be nullptr. Needs 2k < n. */
+umapcu_status umapcu_embedding_quality(const float *x, uint32_t n, uint32_t dim, const float *y, uint32_t n_dim,
+                                       const int32_t *knn_idx, uint32_t knn_k, uint32_t k,
+                                       const uint32_t *queries, uint32_t n_queries, uint32_t metric,
+                                       double *trust, double *knn_preservation);
+
+/* Fuzzy cross-entropy of an embedding against its graph (COO, host):
+ * sum over entries of w log(w/q) + (1-w) log((1-w)/(1-q)),
+ * q = 1 / (1 + a |y_i - y_j|^(2b)), q and w clamped to [1e-12, 1 - 1e-12],
+ * in f64. */
+umapcu_status umapcu_fuzzy_cross_entropy(const uint32_t *row, const uint32_t *col, const float *w, uint64_t nnz,
+                                         const float *y, uint32_t n, uint32_t n_dim, float a, float b,
+                                         double *out);
+
+/* kNN cache file (no reference counterpart: the reference keeps
+ * PreComputedKnn in memory, src/lib.rs:79). Little-endian: a 48-byte header
+ * {"UMAPKNN\0", u32 version = 1, u32 metric, u64 n, u32 k, u32 flags
+ * (bit 0: self excluded), u64 payload checksum (FNV-1a 64 over the payload),
+ * u64 reserved = 0}, then idx i32 [n * k], then dist f32 [n * k]. Loading
+ * checks magic, version, sizes and checksum (UMAPCU_BAD_ARG on mismatch). */
+umapcu_status umapcu_knn_save(const char *path, uint32_t n, uint32_t k, uint32_t metric, const int32_t *knn_idx,
+                              const float *knn_dist);
+umapcu_status umapcu_knn_load_header(const char *path, uint32_t *n, uint32_t *k, uint32_t *metric);
+umapcu_status umapcu_knn_load(const char *path, uint32_t n, uint32_t k, int32_t *knn_idx, float *knn_dist);
+
 #ifdef __cplusplus
 }
 #endif

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -185,6 +186,15 @@ umapcu_status build_csr_multi(uint32_t n_total, uint32_t n_jobs, const uint32_t 
                               const uint64_t *d_job_entry_base, const uint64_t *d_lptr, const uint32_t *d_adj_col,
                               const float *d_adj_w, uint64_t nnz, DeviceCsr &csr, uint64_t *h_job_edges,
                               cudaStream_t s);
+
+// Exact kNN of the rows d_qidx [nq] of d_x (nullptr: rows 0..nq-1), self
+// excluded, ascending (distance, index); knn.cu.
+void knn_dev(const float *d_x, uint32_t n, uint32_t dim, const uint32_t *d_qidx, uint32_t nq, uint32_t k,
+             uint32_t metric, uint32_t *d_idx, float *d_dist, cudaStream_t s);
+// d_counts [nq][k]: points strictly before each given neighbour in the
+// query's (distance, index) order, self excluded; knn.cu.
+void knn_rank_dev(const float *d_x, uint32_t n, uint32_t dim, const uint32_t *d_qidx, uint32_t nq,
+                  const uint32_t *d_nbr, uint32_t k, uint32_t metric, uint32_t *d_counts, cudaStream_t s);
 
 // Resets every entry's schedule cursor to its period (upload state,
 // umap_optimiser_gpu.rs:425-430).

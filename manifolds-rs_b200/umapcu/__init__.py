@@ -142,6 +142,13 @@ _SIGS = {
     "umapcu_server_wait": [_vp, _u64, _vp, _vp, _vp],
     "umapcu_server_stats": [_vp, _vp, _vp, _vp, _vp],
     "umapcu_eval_pow": [_vp, _u32, _f32, _i32, _vp],
+    "umapcu_knn_exact": [_vp, _u32, _u32, _u32, _u32, _vp, _vp],
+    "umapcu_knn_exact_dev": [_vp, _u32, _u32, _vp, _u32, _u32, _u32, _vp, _vp, _vp],
+    "umapcu_embedding_quality": [_vp, _u32, _u32, _vp, _u32, _vp, _u32, _u32, _vp, _u32, _u32, _vp, _vp],
+    "umapcu_fuzzy_cross_entropy": [_vp, _vp, _vp, _u64, _vp, _u32, _u32, _f32, _f32, _vp],
+    "umapcu_knn_save": [C.c_char_p, _u32, _u32, _u32, _vp, _vp],
+    "umapcu_knn_load_header": [C.c_char_p, _vp, _vp, _vp],
+    "umapcu_knn_load": [C.c_char_p, _u32, _u32, _vp, _vp],
 }
 for _name, _args in _SIGS.items():
     _fn = getattr(_lib, _name)
@@ -691,3 +698,78 @@ def sample_negatives(sampler, seed, node, entry, epoch, edge_local, count, n):
     _check(_lib.umapcu_sample_negatives(sampler, seed & (2 ** 64 - 1), node, entry, epoch, edge_local, count, n,
                                         _p(out)))
     return out
+
+
+# ------------------------------------------------------- kNN and metrics
+
+METRIC_EUCLIDEAN_SQ, METRIC_COSINE = 0, 1
+_METRICS = {"euclidean": METRIC_EUCLIDEAN_SQ, "cosine": METRIC_COSINE}
+
+
+def _metric(m) -> int:
+    return _METRICS[m] if isinstance(m, str) else int(m)
+
+
+def knn_exact(data: np.ndarray, k: int, dist_metric="euclidean"):
+    """Exact kNN on the GPU, self excluded -- what run_ann_search with
+    AnnSearch::Exhaustive returns (src/data/nearest_neighbours.rs:225-364):
+    (indices int32 [n, k], distances f32 [n, k]), Euclidean distances
+    squared as the reference's ANN backends return them."""
+    X = _c(data, np.float32)
+    n, dim = X.shape
+    idx = np.empty((n, k), np.int32)
+    dist = np.empty((n, k), np.float32)
+    _check(_lib.umapcu_knn_exact(_p(X), n, dim, k, _metric(dist_metric), _p(idx), _p(dist)), "knn_exact")
+    return idx, dist
+
+
+def embedding_quality(data: np.ndarray, embd: np.ndarray, knn_idx=None, k: int = 15, queries=None,
+                      dist_metric="euclidean"):
+    """trustworthiness@k (sklearn's definition) and kNN preservation@k of an
+    embedding, on the GPU, over the query rows (all rows by default).
+    -> dict(trust=..., knn_preservation=... or None)."""
+    X = _c(data, np.float32)
+    Y = _c(embd, np.float32)
+    n = X.shape[0]
+    q = None if queries is None else _c(queries, np.uint32)
+    ki = None if knn_idx is None else _c(knn_idx, np.int32)
+    t = C.c_double()
+    kp = C.c_double()
+    _check(_lib.umapcu_embedding_quality(_p(X), n, X.shape[1], _p(Y), Y.shape[1], _p(ki),
+                                         0 if ki is None else ki.shape[1], k, _p(q), 0 if q is None else q.size,
+                                         _metric(dist_metric), C.byref(t), None if ki is None else C.byref(kp)),
+           "embedding_quality")
+    return dict(trust=t.value, knn_preservation=None if ki is None else kp.value)
+
+
+def fuzzy_cross_entropy(graph: "CoordinateList", embd: np.ndarray, a: float, b: float) -> float:
+    """Fuzzy cross-entropy of an embedding against its graph, f64, on the GPU."""
+    Y = _c(embd, np.float32)
+    r, c = _c(graph.row_indices, np.uint32), _c(graph.col_indices, np.uint32)
+    w = _c(graph.values, np.float32)
+    out = C.c_double()
+    _check(_lib.umapcu_fuzzy_cross_entropy(_p(r), _p(c), _p(w), r.size, _p(Y), Y.shape[0], Y.shape[1], a, b,
+                                           C.byref(out)), "fuzzy_cross_entropy")
+    return out.value
+
+
+def save_knn(path: str, knn_idx: np.ndarray, knn_dist: np.ndarray, dist_metric="euclidean"):
+    """Writes a kNN cache file (format in umapcu.h)."""
+    i = _c(knn_idx, np.int32)
+    d = _c(knn_dist, np.float32)
+    if i.shape != d.shape or i.ndim != 2:
+        raise ManifoldsError(BAD_ARG, "knn_idx and knn_dist must both be [n, k]")
+    _check(_lib.umapcu_knn_save(os.fsencode(path), i.shape[0], i.shape[1], _metric(dist_metric), _p(i), _p(d)),
+           "knn_save")
+
+
+def load_knn(path: str):
+    """-> (indices int32 [n, k], distances f32 [n, k], metric) from a kNN
+    cache file; checksum and indices are verified."""
+    n, k, m = C.c_uint32(), C.c_uint32(), C.c_uint32()
+    bp = os.fsencode(path)
+    _check(_lib.umapcu_knn_load_header(bp, C.byref(n), C.byref(k), C.byref(m)), "knn_load_header")
+    i = np.empty((n.value, k.value), np.int32)
+    d = np.empty((n.value, k.value), np.float32)
+    _check(_lib.umapcu_knn_load(bp, n.value, k.value, _p(i), _p(d)), "knn_load")
+    return i, d, m.value

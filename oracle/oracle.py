@@ -104,6 +104,11 @@ def lib():
                                               C.c_uint32, C.c_float, C.c_float, C.c_float, vp, C.c_float,
                                               C.c_float, C.c_float, C.c_float, C.c_uint64]
         L.orc_active_edges_per_epoch.argtypes = [f32p, C.c_uint64, C.c_uint32, u64p]
+        L.orc_knn_exact.restype = C.c_int
+        L.orc_knn_exact.argtypes = [f32p, C.c_uint32, C.c_uint32, vp, C.c_uint32, C.c_uint32, C.c_int, u32p, f32p]
+        L.orc_rank_counts.restype = C.c_int
+        L.orc_rank_counts.argtypes = [f32p, C.c_uint32, C.c_uint32, vp, C.c_uint32, u32p, C.c_uint32, C.c_int,
+                                      u32p]
         _lib = L
     return _lib
 
@@ -390,3 +395,53 @@ def active_edges_per_epoch(eps, n_epochs):
     out = np.zeros(n_epochs, np.uint64)
     lib().orc_active_edges_per_epoch(e, e.size, n_epochs, out)
     return out
+
+
+# ------------------------------------------------------- kNN and metrics
+
+def knn_exact(X, k, queries=None, metric=0):
+    """Exact kNN restatement (ann-search-rs exhaustive search as called by
+    nearest_neighbours.rs:313-361): self excluded, sequential-FMA f32
+    distances, ties by index. -> (idx u32 [nq, k], dist f32 [nq, k])."""
+    X = _f32(X)
+    n, dim = X.shape
+    q = None if queries is None else np.ascontiguousarray(queries, np.uint32)
+    nq = n if q is None else q.size
+    idx = np.empty((nq, k), np.uint32)
+    dist = np.empty((nq, k), np.float32)
+    st = lib().orc_knn_exact(X, n, dim, None if q is None else q.ctypes.data, nq, k, metric, idx, dist)
+    if st != OK:
+        raise ValueError(f"orc_knn_exact: status {st}")
+    return idx, dist
+
+
+def rank_counts(X, nbr, queries=None, metric=0):
+    """0-based rank of each given neighbour in its query's (distance, index)
+    order over all other points."""
+    X = _f32(X)
+    n, dim = X.shape
+    nbr = np.ascontiguousarray(nbr, np.uint32)
+    q = None if queries is None else np.ascontiguousarray(queries, np.uint32)
+    nq, k = nbr.shape
+    out = np.empty((nq, k), np.uint32)
+    lib().orc_rank_counts(X, n, dim, None if q is None else q.ctypes.data, nq, nbr, k, metric, out)
+    return out
+
+
+def trustworthiness(X, Y, k=15, queries=None, metric=0):
+    """sklearn.manifold.trustworthiness's definition, restated on the exact
+    kNN above (over a query subset: the same sum over those queries, the
+    normalisation with their count)."""
+    n = X.shape[0]
+    ynbr, _ = knn_exact(Y, k, queries)
+    c = rank_counts(X, ynbr, queries, metric).astype(np.float64)
+    nq = ynbr.shape[0]
+    pen = np.maximum(0.0, c + 1.0 - k).sum()
+    return 1.0 - pen * (2.0 / (nq * k * (2.0 * n - 3.0 * k - 1.0)))
+
+
+def knn_preservation(knn_idx, Y, k=15, queries=None):
+    ynbr, _ = knn_exact(Y, k, queries)
+    rows = np.arange(Y.shape[0]) if queries is None else np.asarray(queries)
+    kx = np.asarray(knn_idx)[rows, :k]
+    return float(np.mean([len(set(a.tolist()) & set(b.tolist())) / k for a, b in zip(kx, ynbr)]))

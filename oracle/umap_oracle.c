@@ -1192,3 +1192,115 @@ void orc_active_edges_per_epoch(const float *eps, uint64_t n_edges, uint32_t n_e
         free(loc);
     }
 }
+
+/* ------------------------------------------------ exact kNN and ranks
+ * The reference's exact search is ann-search-rs 0.5.2's exhaustive index
+ * (third-party, not vendored; called from src/data/nearest_neighbours.rs:
+ * 313-316 with k + 1, the first result -- self -- dropped at :352-361). Its
+ * published algorithm: every point against every query, the k smallest
+ * squared Euclidean (or cosine) distances. Restated here with the
+ * arithmetic fixed so that results are reproducible bit for bit: each
+ * distance is the sequential f32 FMA chain over dimensions in order, ties are
+ * broken by the smaller index, self (the query's own row) is excluded. */
+
+static inline int orc_better(float d, uint32_t i, float td, uint32_t ti)
+{
+    return d < td || (d == td && i < ti);
+}
+
+static void orc_unit_rows(const float *x, uint32_t n, uint32_t dim, float *xn)
+{
+    for (uint32_t i = 0; i < n; i++) {
+        const float *r = x + (size_t)i * dim;
+        float s = 0.0f;
+        for (uint32_t d = 0; d < dim; d++) s = fmaf(r[d], r[d], s);
+        const float nrm = sqrtf(s);
+        for (uint32_t d = 0; d < dim; d++) xn[(size_t)i * dim + d] = nrm > 0.0f ? r[d] / nrm : 0.0f;
+    }
+}
+
+static inline float orc_dist(const float *a, const float *b, uint32_t dim, int metric)
+{
+    float s = 0.0f;
+    if (metric == 0) {
+        for (uint32_t d = 0; d < dim; d++) {
+            const float df = a[d] - b[d];
+            s = fmaf(df, df, s);
+        }
+        return s;
+    }
+    for (uint32_t d = 0; d < dim; d++) s = fmaf(a[d], b[d], s);
+    return 1.0f - s;
+}
+
+/* metric 0: squared Euclidean, 1: cosine (1 - <x/|x|, y/|y|>). qidx NULL:
+ * queries are rows 0..nq-1. idx/dist [nq * k], ascending. */
+int orc_knn_exact(const float *x, uint32_t n, uint32_t dim, const uint32_t *qidx, uint32_t nq, uint32_t k,
+                  int metric, uint32_t *idx, float *dist)
+{
+    if (n == 0) return ORC_NO_DATA;
+    if (k == 0 || n <= k) return ORC_BAD_ARG;
+    const float *xs = x;
+    float *xn = NULL;
+    if (metric == 1) {
+        xn = (float *)malloc(sizeof(float) * (size_t)n * dim);
+        orc_unit_rows(x, n, dim, xn);
+        xs = xn;
+    }
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t q = 0; q < (int64_t)nq; q++) {
+        const uint32_t gq = qidx ? qidx[q] : (uint32_t)q;
+        float *ld = dist + (size_t)q * k;
+        uint32_t *li = idx + (size_t)q * k;
+        for (uint32_t m = 0; m < k; m++) {
+            ld[m] = INFINITY;
+            li[m] = UINT32_MAX;
+        }
+        for (uint32_t p = 0; p < n; p++) {
+            if (p == gq) continue;
+            const float d = orc_dist(xs + (size_t)gq * dim, xs + (size_t)p * dim, dim, metric);
+            if (!orc_better(d, p, ld[k - 1], li[k - 1])) continue;
+            uint32_t m = k - 1;
+            while (m > 0 && orc_better(d, p, ld[m - 1], li[m - 1])) {
+                ld[m] = ld[m - 1];
+                li[m] = li[m - 1];
+                m--;
+            }
+            ld[m] = d;
+            li[m] = p;
+        }
+    }
+    free(xn);
+    return ORC_OK;
+}
+
+/* counts[q][m] = #{p != query : (d(q,p), p) strictly before (d(q,nbr), nbr)}
+ * for nbr = nbr[q][m] -- the 0-based rank of that neighbour. */
+int orc_rank_counts(const float *x, uint32_t n, uint32_t dim, const uint32_t *qidx, uint32_t nq,
+                    const uint32_t *nbr, uint32_t k, int metric, uint32_t *counts)
+{
+    const float *xs = x;
+    float *xn = NULL;
+    if (metric == 1) {
+        xn = (float *)malloc(sizeof(float) * (size_t)n * dim);
+        orc_unit_rows(x, n, dim, xn);
+        xs = xn;
+    }
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t q = 0; q < (int64_t)nq; q++) {
+        const uint32_t gq = qidx ? qidx[q] : (uint32_t)q;
+        float td[64];
+        for (uint32_t m = 0; m < k && m < 64; m++) {
+            td[m] = orc_dist(xs + (size_t)gq * dim, xs + (size_t)nbr[(size_t)q * k + m] * dim, dim, metric);
+            counts[(size_t)q * k + m] = 0;
+        }
+        for (uint32_t p = 0; p < n; p++) {
+            if (p == gq) continue;
+            const float d = orc_dist(xs + (size_t)gq * dim, xs + (size_t)p * dim, dim, metric);
+            for (uint32_t m = 0; m < k && m < 64; m++)
+                counts[(size_t)q * k + m] += orc_better(d, p, td[m], nbr[(size_t)q * k + m]);
+        }
+    }
+    free(xn);
+    return ORC_OK;
+}
