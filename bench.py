@@ -68,11 +68,44 @@ def log(*a):
 
 # ----------------------------------------------------------------- inputs
 
-def make_problem(wl, seed, device_knn=True, reference_graph=False):
-    """Synthetic data -> exact kNN (input preparation: the library's GPU
-    kernel for the umapcu arm, torch for the reference arm) -> fuzzy graph:
-    the CUDA graph stage for the umapcu arm, the oracle's CPU restatement of
-    the reference's graph stage for the reference arm."""
+def knn_cache_path(wl, seed):
+    d = os.environ.get("UMAPCU_KNN_CACHE") or os.path.join(__import__("tempfile").gettempdir(), "umapcu_knn")
+    os.makedirs(d, exist_ok=True)
+    return os.path.join(d, f"{wl['kind']}_n{wl['n']}_d{wl['dim']}_c{wl['clusters']}_k{wl['k']}_s{seed}.knn")
+
+
+def shared_knn(X, wl, seed):
+    """The workload's exact kNN, computed once and cached (kNN cache file)
+    as the shared input of both arms: input preparation, outside every timed
+    region. Computed by the library's exact GPU kNN when a GPU is present,
+    else by the CPU brute force; both are exact (ties by index)."""
+    import umapcu
+    path = knn_cache_path(wl, seed)
+    if os.path.exists(path):
+        try:
+            idx, dist, _ = umapcu.load_knn(path)
+            if idx.shape == (wl["n"], wl["k"]):
+                log(f"[bench] kNN from cache {path}")
+                return idx, dist
+        except umapcu.ManifoldsError:
+            pass
+    import torch
+    if torch.cuda.is_available():
+        idx, dist = umapcu.knn_exact(X, wl["k"])
+    else:
+        import umapcu.synth as S
+        idx, dist = S.exact_knn_cpu(X, wl["k"])
+        idx, dist = idx.astype(np.int32), dist.astype(np.float32)
+    tmp = f"{path}.{os.getpid()}.tmp"
+    umapcu.save_knn(tmp, idx, dist)
+    os.replace(tmp, path)
+    return idx, dist
+
+
+def make_problem(wl, seed, reference_graph=False):
+    """Synthetic data -> exact kNN (shared cached input) -> fuzzy graph: the
+    CUDA graph stage for the umapcu arm, the oracle's CPU restatement of the
+    reference's graph stage for the reference arm."""
     import umapcu
     import umapcu.synth as S
     t0 = time.time()
@@ -82,10 +115,7 @@ def make_problem(wl, seed, device_knn=True, reference_graph=False):
         X, _ = S.variable_density_mixture(wl["n"], wl["dim"], wl["clusters"], seed)
     else:
         X, _ = S.isotropic_mixture(wl["n"], wl["dim"], wl["clusters"], seed)
-    if reference_graph:
-        idx, dist = S.exact_knn_torch(X, wl["k"]) if device_knn else S.exact_knn_cpu(X, wl["k"])
-    else:
-        idx, dist = umapcu.knn_exact(X, wl["k"])
+    idx, dist = shared_knn(X, wl, seed)
     t1 = time.time()
     if reference_graph:
         from oracle import oracle as O
@@ -567,10 +597,8 @@ def run_served(args, wl, world, rank, local_rank):
 def run_reference(args, wl, world):
     """The reference's parallel-Adam CPU optimiser on the host cores,
     bounded windows of the same workload (one window per step)."""
-    import torch
     seed = args.seed
-    have_gpu = torch.cuda.is_available()
-    prob = make_problem(wl, seed, device_knn=have_gpu, reference_graph=True)
+    prob = make_problem(wl, seed, reference_graph=True)
     from oracle import oracle as O
     adj = prob["adj"]
     stt, csr = O.csr_from_graph(wl["n"], adj.ptr, adj.col, adj.w)
