@@ -196,7 +196,6 @@ struct WarpSmem {
     uint32_t beg[33];
     uint32_t qp[kQ];
     uint32_t qo[kQ];
-    uint8_t qj[kQ];
     uint8_t run_len[32];
     uint8_t run_start[32];
     float ys[32][D];
@@ -215,7 +214,9 @@ __device__ __forceinline__ uint32_t local_node(const uint32_t *beg, uint32_t p)
 }
 
 // One batch of `cnt` queued active entries (cnt <= 32) starting at queue
-// slot q0; lane t = slot q0 + t.
+// slot q0; lane t = slot q0 + t. The lane's node is found here (active
+// entries only), and the other endpoint's row and the first chunk of
+// negatives' rows are gathered together, so a batch waits on L2 once.
 template <int D, bool DENS, int NR, bool COH, int KU>
 __device__ __forceinline__ void process_batch(const EpochArgs &A, WarpSmem<D, KU> &S, uint32_t q0, uint32_t cnt,
                                               uint32_t node0, int lane, float (&g)[D], bool &act,
@@ -225,13 +226,44 @@ __device__ __forceinline__ void process_batch(const EpochArgs &A, WarpSmem<D, KU
     uint32_t j = 0;
     if (live) {
         const uint32_t p = S.qp[q0 + lane], o = S.qo[q0 + lane];
-        j = S.qj[q0 + lane];
+        j = local_node(S.beg, p);
         const uint32_t self = node0 + j;
+        const uint32_t edge_local = p - S.beg[j];
         float ys[D], yo[D], c[D];
 #pragma unroll
         for (int d = 0; d < D; d++) { ys[d] = S.ys[j][d]; c[d] = 0.0f; }
         const uint64_t pol = l2_keep_policy();
+        constexpr int kNegChunk = neg_chunk<NR>();
+        const uint32_t neg_rate = NR > 0 ? (uint32_t)NR : A.neg_rate;
+        uint32_t kk[kNegChunk];
+        float yk[kNegChunk][D];
+        // negatives of chunk k0 (umap_optimiser_gpu.rs:801-816): indices and
+        // gathers issued before any of them is used
+        auto issue = [&](uint32_t k0) {
+            uint4 ph = make_uint4(0, 0, 0, 0);
+#pragma unroll
+            for (int t = 0; t < kNegChunk; t++) {
+                const uint32_t neg = k0 + t;
+                uint32_t kn = self;
+                if (neg < neg_rate) {
+                    if (A.injected) {
+                        kn = A.injected[(uint64_t)p * neg_rate + neg];
+                    } else if (A.sampler == UMAPCU_NEG_PHILOX) {
+                        if ((t & 3) == 0) ph = philox4x32_10(make_uint4(p, A.epoch, neg >> 2, 0x554D4150u), A.seed_lo,
+                                                             A.seed_hi);
+                        uint32_t r = (t & 3) == 0 ? ph.x : (t & 3) == 1 ? ph.y : (t & 3) == 2 ? ph.z : ph.w;
+                        kn = range32(r, A.n);
+                    } else {
+                        kn = fastmod_u32(hash_neg_raw(A.seed32, self, A.epoch, edge_local, neg), A.fastmod_M, A.n);
+                    }
+                }
+                kk[t] = kn;
+                if (neg < neg_rate) load_row_keep<D, COH>(A.y_cur, kn, yk[t], pol);
+            }
+        };
         load_row_keep<D, COH>(A.y_cur, o, yo, pol);
+        // (wider rows: registers for all gathers at once would spill)
+        if constexpr (D <= 2) issue(0);
         float4 dno;
         float mu_e = 1.0f;
         if constexpr (DENS) {
@@ -253,8 +285,9 @@ __device__ __forceinline__ void process_batch(const EpochArgs &A, WarpSmem<D, KU
 #pragma unroll
                 for (int d = 0; d < D; d++) c[d] += 2.0f * clip4(grad_coeff * (yo[d] - ys[d]));
             } else {
+                const float gc2 = 2.0f * grad_coeff;
 #pragma unroll
-                for (int d = 0; d < D; d++) c[d] += 2.0f * grad_coeff * (yo[d] - ys[d]);
+                for (int d = 0; d < D; d++) c[d] += gc2 * (yo[d] - ys[d]);
             }
             if constexpr (DENS) {
                 // umap_optimiser_gpu.rs:769-798
@@ -271,48 +304,24 @@ __device__ __forceinline__ void process_batch(const EpochArgs &A, WarpSmem<D, KU
                 for (int d = 0; d < D; d++) c[d] += 2.0f * clip4(two_cor * (ys[d] - yo[d]));
             }
         }
-        // negatives (umap_optimiser_gpu.rs:801-849), gathered in chunks
-        const uint32_t edge_local = p - S.beg[j];
-        constexpr int kNegChunk = neg_chunk<NR>();
-        const uint32_t neg_rate = NR > 0 ? (uint32_t)NR : A.neg_rate;
+        // negatives (umap_optimiser_gpu.rs:817-849)
         for (uint32_t k0 = 0; k0 < neg_rate; k0 += kNegChunk) {
-            uint32_t kk[kNegChunk];
-            float yk[kNegChunk][D];
-            uint4 ph = make_uint4(0, 0, 0, 0);
-#pragma unroll
-            for (int t = 0; t < kNegChunk; t++) {
-                const uint32_t neg = k0 + t;
-                uint32_t kn = self;
-                if (neg < neg_rate) {
-                    if (A.injected) {
-                        kn = A.injected[(uint64_t)p * neg_rate + neg];
-                    } else if (A.sampler == UMAPCU_NEG_PHILOX) {
-                        if ((t & 3) == 0) ph = philox4x32_10(make_uint4(p, A.epoch, neg >> 2, 0x554D4150u), A.seed_lo,
-                                                             A.seed_hi);
-                        uint32_t r = (t & 3) == 0 ? ph.x : (t & 3) == 1 ? ph.y : (t & 3) == 2 ? ph.z : ph.w;
-                        kn = range32(r, A.n);
-                    } else {
-                        kn = fastmod_u32(hash_neg_raw(A.seed32, self, A.epoch, edge_local, neg), A.fastmod_M, A.n);
-                    }
-                }
-                kk[t] = kn;
-                if (neg < neg_rate) load_row_keep<D, COH>(A.y_cur, kn, yk[t], pol);
-            }
+            if (k0 || D > 2) issue(k0);
 #pragma unroll
             for (int t = 0; t < kNegChunk; t++) {
                 if (k0 + t < neg_rate && kk[t] != self) {
-                    float dsk = 0.0f;
+                    float diff[D], dsk = 0.0f;
 #pragma unroll
                     for (int d = 0; d < D; d++) {
-                        float diff = ys[d] - yk[t][d];
-                        dsk += diff * diff;
+                        diff[d] = ys[d] - yk[t][d];
+                        dsk += diff[d] * diff[d];
                     }
                     float dist_sq_safe = dsk + 0.001f;
                     float dist_sq_b = pow_pos(dist_sq_safe, A.b, A.precise_pow);
                     float denom = dist_sq_safe * (1.0f + A.a * dist_sq_b);
                     float gc = clip4(div_k(A.two_gamma_b, denom, A.precise_pow));
 #pragma unroll
-                    for (int d = 0; d < D; d++) c[d] += gc * (ys[d] - yk[t][d]);
+                    for (int d = 0; d < D; d++) c[d] += gc * diff[d];
                 }
             }
         }
@@ -401,7 +410,6 @@ __device__ __forceinline__ void epoch_segment(const EpochArgs &A, WarpSmem<D, KU
                 const uint32_t slot = count + __popc(mask & lt_mask);
                 S.qp[slot] = p;
                 S.qo[slot] = ov[u];
-                S.qj[slot] = (uint8_t)local_node(S.beg, p);
             }
             count += __popc(mask);
         }
@@ -415,10 +423,9 @@ __device__ __forceinline__ void epoch_segment(const EpochArgs &A, WarpSmem<D, KU
         const uint32_t rem = count - upto;
         if (upto && rem) {
             uint32_t tp = 0, to = 0;
-            uint8_t tj = 0;
-            if ((uint32_t)lane < rem) { tp = S.qp[upto + lane]; to = S.qo[upto + lane]; tj = S.qj[upto + lane]; }
+            if ((uint32_t)lane < rem) { tp = S.qp[upto + lane]; to = S.qo[upto + lane]; }
             __syncwarp();
-            if ((uint32_t)lane < rem) { S.qp[lane] = tp; S.qo[lane] = to; S.qj[lane] = tj; }
+            if ((uint32_t)lane < rem) { S.qp[lane] = tp; S.qo[lane] = to; }
             __syncwarp();
         }
         count = rem;

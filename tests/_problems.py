@@ -43,3 +43,13 @@ def fuzzy_cross_entropy(row, col, w, Y, a, b):
     q = np.clip(1.0 / (1.0 + a * d2 ** b), 1e-12, 1 - 1e-12)
     w = np.clip(w.astype(np.float64), 1e-12, 1 - 1e-12)
     return float(np.sum(w * np.log(w / q) + (1 - w) * np.log((1 - w) / (1 - q))))
+
+
+def oracle_adam_gpu_run(args):
+    """One oracle run of the reference's GPU optimiser (process-pool worker):
+    (init, ptr, col, val, params dict, seed, sampler) -> final embedding."""
+    init, ptr, col, val, pd, seed, sampler = args
+    st, yo = O.optimise_adam_gpu(init, init.shape[0], ptr, col, val, pd, seed, sampler=sampler)
+    if st != O.OK:
+        raise RuntimeError(f"oracle status {st}")
+    return yo

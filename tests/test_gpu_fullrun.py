@@ -1,23 +1,42 @@
 """Full layout runs: the CUDA optimiser vs the oracle's restatement of the
-reference's GPU optimiser (same graph, same initial embedding, same seed and
-the reference's own negative-sample hash). The trajectories diverge
-chaotically at the f32 rounding level, so the bar is on the final quality
-metrics: trustworthiness@15, kNN preservation@15 and the fuzzy cross-entropy
-of the graph under the embedding, each within 1 % (north-star parity bar)."""
+reference's GPU optimiser (same graph, same initial embedding, the
+reference's own negative-sample hash or the Philox sampler on both sides).
+Trajectories diverge chaotically at the f32 rounding level, and the final
+metrics then vary from seed to seed for the reference itself (measured on
+this problem: kNN preservation std 1.2 %, fuzzy cross-entropy std 1.4 %, a
+4 % spread over five seeds), so one run per side cannot separate a 1 %
+difference from seed noise. The north-star bar -- trustworthiness@15, kNN
+preservation@15 and fuzzy cross-entropy within 1 % -- is applied to the
+means over 32 seeds per side (two disjoint 32-seed sets of the oracle agree
+to 0.02 % / 0.13 % / 0.02 %)."""
+import multiprocessing as mp
+import os
+from concurrent.futures import ProcessPoolExecutor
+
 import numpy as np
 import pytest
 
 from oracle import oracle as O
-from tests._problems import fuzzy_cross_entropy, knn_preservation, oracle_graph
+from tests._problems import fuzzy_cross_entropy, knn_preservation, oracle_adam_gpu_run, oracle_graph
 
 pytestmark = pytest.mark.gpu
 
 umapcu = pytest.importorskip("umapcu")
 
+N_SEEDS = 32
+
 
 def _metrics(g, Y, p):
     from sklearn.manifold import trustworthiness
     return dict(trust=trustworthiness(g["X"], Y, n_neighbors=15), knn=knn_preservation(g["idx"], Y),
+                ce=fuzzy_cross_entropy(g["row"], g["col"], g["val"], Y, p.a, p.b))
+
+
+def _metrics_gpu(g, Y, p):
+    """Same definitions, on the device (the metric kernels are pinned to
+    sklearn and the oracle in test_gpu_knn.py)."""
+    q = umapcu.embedding_quality(g["X"], Y, g["idx"].astype(np.int32), 15)
+    return dict(trust=q["trust"], knn=q["knn_preservation"],
                 ce=fuzzy_cross_entropy(g["row"], g["col"], g["val"], Y, p.a, p.b))
 
 
@@ -31,23 +50,51 @@ def c1_small():
     return oracle_graph(n=5000, dim=50, k=15, clusters=10, seed=1, n_epochs=500, kind="subspace")
 
 
+def _params():
+    return umapcu.UmapOptimParams.from_min_dist_spread(0.1, 1.0, n_epochs=500, neg_sample_rate=5)
+
+
+def _oracle_ensemble(g, init, p, sampler):
+    """The oracle's runs for seeds 0..N_SEEDS-1, one process per run
+    (spawned, single-threaded each)."""
+    jobs = [(init, g["ptr"], g["col"], g["val"], p.as_dict(), s, sampler) for s in range(N_SEEDS)]
+    old = os.environ.get("OMP_NUM_THREADS")
+    os.environ["OMP_NUM_THREADS"] = "1"
+    try:
+        with ProcessPoolExecutor(min(16, os.cpu_count() or 1), mp_context=mp.get_context("spawn")) as ex:
+            return list(ex.map(oracle_adam_gpu_run, jobs))
+    finally:
+        if old is None:
+            del os.environ["OMP_NUM_THREADS"]
+        else:
+            os.environ["OMP_NUM_THREADS"] = old
+
+
 @pytest.mark.parametrize("sampler", ["ref_hash", "philox"])
 def test_full_run_quality_matches_reference(c1_small, sampler):
     g = c1_small
     n = 5000
-    p = umapcu.UmapOptimParams.from_min_dist_spread(0.1, 1.0, n_epochs=500, neg_sample_rate=5)
+    p = _params()
     init = umapcu.random_layout(n, 2, 17)
     adj = umapcu.Adjacency(g["ptr"], g["col"], g["val"])
-    y = init.copy()
     smp = umapcu.NEG_PHILOX if sampler == "philox" else umapcu.NEG_REF_HASH
-    umapcu.optimise_embedding_adam_gpu(y, adj, p, None, 42, 0, smp)
-    st, yo = O.optimise_adam_gpu(init, n, g["ptr"], g["col"], g["val"], p.as_dict(), 42,
-                                 sampler=O.SAMPLER_PHILOX if sampler == "philox" else O.SAMPLER_HASH)
-    assert st == O.OK and np.isfinite(y).all()
-    mg, mo = _metrics(g, y, p), _metrics(g, yo, p)
+    ys = []
+    for s in range(N_SEEDS):
+        y = init.copy()
+        umapcu.optimise_embedding_adam_gpu(y, adj, p, None, s, 0, smp)
+        assert np.isfinite(y).all()
+        ys.append(y)
+    yos = _oracle_ensemble(g, init, p, O.SAMPLER_PHILOX if sampler == "philox" else O.SAMPLER_HASH)
+    mg = [_metrics_gpu(g, y, p) for y in ys]
+    mo = [_metrics_gpu(g, y, p) for y in yos]
     for key in ("trust", "knn", "ce"):
-        assert abs(mg[key] - mo[key]) <= 0.01 * abs(mo[key]), (key, mg[key], mo[key])
-    assert mg["trust"] > 0.9
+        a = float(np.mean([m[key] for m in mg]))
+        b = float(np.mean([m[key] for m in mo]))
+        assert abs(a - b) <= 0.01 * abs(b), (key, a, b)
+    assert np.mean([m["trust"] for m in mg]) > 0.9
+    # one pair on sklearn's own implementation as well
+    m1, m2 = _metrics(g, ys[0], p), _metrics(g, yos[0], p)
+    assert abs(m1["trust"] - m2["trust"]) <= 0.01 * m2["trust"]
 
 
 def test_gpu_sgd_full_run_quality(c1_small):
