@@ -196,8 +196,6 @@ struct WarpSmem {
     uint32_t beg[33];
     uint32_t qp[kQ];
     uint32_t qo[kQ];
-    uint8_t run_len[32];
-    uint8_t run_start[32];
     float ys[32][D];
     float part[32][D];
     float4 dn[32];
@@ -217,21 +215,27 @@ __device__ __forceinline__ uint32_t local_node(const uint32_t *beg, uint32_t p)
 // slot q0; lane t = slot q0 + t. The lane's node is found here (active
 // entries only), and the other endpoint's row and the first chunk of
 // negatives' rows are gathered together, so a batch waits on L2 once.
-template <int D, bool DENS, int NR, bool COH, int KU>
+// FAST: the common configuration resolved at compile time (reference hash
+// sampler, no injected negatives, MUFU x^b and approximate division), which
+// removes the per-negative and per-term uniform branches of the general path.
+template <int D, bool DENS, int NR, bool COH, int KU, bool FAST>
 __device__ __forceinline__ void process_batch(const EpochArgs &A, WarpSmem<D, KU> &S, uint32_t q0, uint32_t cnt,
                                               uint32_t node0, int lane, float (&g)[D], bool &act,
                                               const float *dstat)
 {
     const bool live = (uint32_t)lane < cnt;
-    uint32_t j = 0;
+    uint32_t j = 32;  // dead lanes: a node of their own, contributing zero
+    float c[D];
+#pragma unroll
+    for (int d = 0; d < D; d++) c[d] = 0.0f;
     if (live) {
         const uint32_t p = S.qp[q0 + lane], o = S.qo[q0 + lane];
         j = local_node(S.beg, p);
         const uint32_t self = node0 + j;
         const uint32_t edge_local = p - S.beg[j];
-        float ys[D], yo[D], c[D];
+        float ys[D], yo[D];
 #pragma unroll
-        for (int d = 0; d < D; d++) { ys[d] = S.ys[j][d]; c[d] = 0.0f; }
+        for (int d = 0; d < D; d++) ys[d] = S.ys[j][d];
         const uint64_t pol = l2_keep_policy();
         constexpr int kNegChunk = neg_chunk<NR>();
         const uint32_t neg_rate = NR > 0 ? (uint32_t)NR : A.neg_rate;
@@ -246,9 +250,9 @@ __device__ __forceinline__ void process_batch(const EpochArgs &A, WarpSmem<D, KU
                 const uint32_t neg = k0 + t;
                 uint32_t kn = self;
                 if (neg < neg_rate) {
-                    if (A.injected) {
+                    if (!FAST && A.injected) {
                         kn = A.injected[(uint64_t)p * neg_rate + neg];
-                    } else if (A.sampler == UMAPCU_NEG_PHILOX) {
+                    } else if (!FAST && A.sampler == UMAPCU_NEG_PHILOX) {
                         if ((t & 3) == 0) ph = philox4x32_10(make_uint4(p, A.epoch, neg >> 2, 0x554D4150u), A.seed_lo,
                                                              A.seed_hi);
                         uint32_t r = (t & 3) == 0 ? ph.x : (t & 3) == 1 ? ph.y : (t & 3) == 2 ? ph.z : ph.w;
@@ -278,9 +282,9 @@ __device__ __forceinline__ void process_batch(const EpochArgs &A, WarpSmem<D, KU
             dist_sq += diff * diff;
         }
         if (dist_sq >= 1e-8f) {
-            float dist_sq_b = pow_pos(dist_sq, A.b, A.precise_pow);
+            float dist_sq_b = pow_pos(dist_sq, A.b, (!FAST && A.precise_pow));
             float denom = 1.0f + A.a * dist_sq_b;
-            float grad_coeff = div_k(A.two_a_b * dist_sq_b, dist_sq * denom, A.precise_pow);
+            float grad_coeff = div_k(A.two_a_b * dist_sq_b, dist_sq * denom, (!FAST && A.precise_pow));
             if (A.optimiser == UMAPCU_OPT_SGD) {
 #pragma unroll
                 for (int d = 0; d < D; d++) c[d] += 2.0f * clip4(grad_coeff * (yo[d] - ys[d]));
@@ -317,44 +321,49 @@ __device__ __forceinline__ void process_batch(const EpochArgs &A, WarpSmem<D, KU
                         dsk += diff[d] * diff[d];
                     }
                     float dist_sq_safe = dsk + 0.001f;
-                    float dist_sq_b = pow_pos(dist_sq_safe, A.b, A.precise_pow);
+                    float dist_sq_b = pow_pos(dist_sq_safe, A.b, (!FAST && A.precise_pow));
                     float denom = dist_sq_safe * (1.0f + A.a * dist_sq_b);
-                    float gc = clip4(div_k(A.two_gamma_b, denom, A.precise_pow));
+                    float gc = clip4(div_k(A.two_gamma_b, denom, (!FAST && A.precise_pow)));
 #pragma unroll
                     for (int d = 0; d < D; d++) c[d] += gc * diff[d];
                 }
             }
         }
-#pragma unroll
-        for (int d = 0; d < D; d++) S.part[lane][d] = c[d];
     }
-    // run of slots per node (slots are sorted by local node)
-    S.run_len[lane] = 0;
-    __syncwarp();
-    const unsigned live_mask = __ballot_sync(kFull, live);
-    if (live) {
-        unsigned same = __match_any_sync(live_mask, j);
-        if (lane == __ffs(same) - 1) {
-            S.run_start[j] = (uint8_t)lane;
-            S.run_len[j] = (uint8_t)__popc(same);
+    // Per-node sums of the lanes' partials: the slots are sorted by node, so
+    // each node's slots form a run; a segmented inclusive scan over the warp
+    // leaves each run's sum on its last lane, which hands it to the node's
+    // lane through shared memory.
+    const uint32_t jprev = __shfl_up_sync(kFull, j, 1);
+    const uint32_t jnext = __shfl_down_sync(kFull, j, 1);
+    const unsigned heads = __ballot_sync(kFull, lane == 0 || jprev != j);
+    const int start = 31 - __clz(heads & (lane == 31 ? kFull : ((2u << lane) - 1u)));
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+#pragma unroll
+        for (int d = 0; d < D; d++) {
+            const float v = __shfl_up_sync(kFull, c[d], off);
+            if (lane - off >= start) c[d] += v;
         }
     }
+    const bool tail = live && (lane == 31 || jnext != j);
+    if (tail) {
+#pragma unroll
+        for (int d = 0; d < D; d++) S.part[j][d] = c[d];
+    }
+    const unsigned has = __reduce_or_sync(kFull, tail ? (1u << j) : 0u);
     __syncwarp();
-    const uint32_t len = S.run_len[lane];
-    if (len) {
+    if ((has >> lane) & 1u) {
         act = true;
-        const uint32_t s0 = S.run_start[lane];
-        for (uint32_t s = s0; s < s0 + len; s++) {
 #pragma unroll
-            for (int d = 0; d < D; d++) g[d] += S.part[s][d];
-        }
+        for (int d = 0; d < D; d++) g[d] += S.part[lane][d];
     }
     __syncwarp();
 }
 
 // One epoch of one 32-node segment [node0, node0 + 32) of problem A, run by
 // one warp (see the file comment).
-template <int D, bool DENS, int NR, bool COH, int KU = kU>
+template <int D, bool DENS, int NR, bool COH, int KU = kU, bool FAST = false>
 __device__ __forceinline__ void epoch_segment(const EpochArgs &A, WarpSmem<D, KU> &S, uint32_t node0, int lane)
 {
     __syncwarp();  // the warp's shared memory may still be read by its previous segment
@@ -419,7 +428,7 @@ __device__ __forceinline__ void epoch_segment(const EpochArgs &A, WarpSmem<D, KU
         const bool last = !more;
         const uint32_t upto = last ? count : (count & ~31u);
         for (uint32_t q0 = 0; q0 < upto; q0 += 32)
-            process_batch<D, DENS, NR, COH, KU>(A, S, q0, min(32u, upto - q0), node0, lane, g, act, dstat);
+            process_batch<D, DENS, NR, COH, KU, FAST>(A, S, q0, min(32u, upto - q0), node0, lane, g, act, dstat);
         const uint32_t rem = count - upto;
         if (upto && rem) {
             uint32_t tp = 0, to = 0;

@@ -36,14 +36,14 @@
 
 namespace umapcu {
 
-template <int D, bool DENS, int NR>
-__global__ void __launch_bounds__(kWarps * 32, 8) k_epoch(const EpochArgs A)
+template <int D, bool DENS, int NR, bool FAST = false>
+__global__ void __launch_bounds__(kWarps * 32, 6) k_epoch(const EpochArgs A)
 {
     __shared__ WarpSmem<D> smem[kWarps];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t node0 = (blockIdx.x * kWarps + warp) * 32u;
     if (node0 >= A.n) return;
-    epoch_segment<D, DENS, NR, false>(A, smem[warp], node0, lane);
+    epoch_segment<D, DENS, NR, false, kU, FAST>(A, smem[warp], node0, lane);
 }
 
 // ------------------------------------------------------------ densMAP
@@ -189,7 +189,9 @@ template <int D, bool DENS>
 static void launch_epoch_t(const EpochArgs &A, cudaStream_t s)
 {
     const uint32_t nseg = ceil_div(A.n, 32);
-    if (A.neg_rate == 5) k_epoch<D, DENS, 5><<<ceil_div(nseg, kWarps), kWarps * 32, 0, s>>>(A);
+    const bool fast = !A.injected && A.sampler == UMAPCU_NEG_REF_HASH && !A.precise_pow;
+    if (A.neg_rate == 5 && fast) k_epoch<D, DENS, 5, true><<<ceil_div(nseg, kWarps), kWarps * 32, 0, s>>>(A);
+    else if (A.neg_rate == 5) k_epoch<D, DENS, 5><<<ceil_div(nseg, kWarps), kWarps * 32, 0, s>>>(A);
     else k_epoch<D, DENS, 0><<<ceil_div(nseg, kWarps), kWarps * 32, 0, s>>>(A);
 }
 
