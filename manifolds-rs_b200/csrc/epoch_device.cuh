@@ -40,8 +40,11 @@ __device__ __forceinline__ uint32_t hash_neg_raw(uint32_t seed, uint32_t node, u
 
 __device__ __forceinline__ uint32_t fastmod_u32(uint32_t a, uint64_t M, uint32_t d)
 {
-    uint64_t lowbits = M * a;
-    return (uint32_t)__umul64hi(lowbits, d);
+    // lowbits = (M * a) mod 2^64, then floor(lowbits * d / 2^64) with d < 2^32:
+    // high word of (lowbits_hi * d + umulhi(lowbits_lo, d)).
+    const uint64_t lowbits = M * a;
+    const uint32_t lo = (uint32_t)lowbits, hi = (uint32_t)(lowbits >> 32);
+    return (uint32_t)(((uint64_t)hi * d + __umulhi(lo, d)) >> 32);
 }
 
 // Philox4x32-10 (Salmon, Moraes, Dror & Shaw, SC'11).
