@@ -244,6 +244,7 @@ def main():
     ap.add_argument("--impl", default="umapcu", choices=["umapcu", "reference"])
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
     ap.add_argument("--sampler", default="ref_hash", choices=["ref_hash", "philox"])
+    ap.add_argument("--optimiser", default="adam", choices=["adam", "sgd"])
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--cpu-seconds", type=float, default=8.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -281,6 +282,7 @@ def main():
     seed = args.seed + rank
     prob = make_problem(wl, seed)
     sampler = umapcu.NEG_PHILOX if args.sampler == "philox" else umapcu.NEG_REF_HASH
+    opt = umapcu.OPT_SGD if args.optimiser == "sgd" else umapcu.OPT_ADAM
     st = umapcu.UmapGpuState(prob["init"], prob["adj"], prob["params"], prob["dens"], seed, sampler)
     E = st.n_edges
     csr = st.csr()
@@ -295,14 +297,14 @@ def main():
     if args.profile_only:
         # a short run for ncu captures: 40 epochs (capture e.g. launch 31)
         st.reset(prob["init"])
-        st.run(0, min(n_ep, 40))
+        st.run(0, min(n_ep, 40), opt)
         torch.cuda.synchronize()
         log("[bench] profile-only run done")
         return
 
     for _ in range(args.warmup):
         st.reset(prob["init"])
-        st.run(0, n_ep)
+        st.run(0, n_ep, opt)
     torch.cuda.synchronize()
 
     times = []
@@ -316,7 +318,7 @@ def main():
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            st.run(0, n_ep)
+            st.run(0, n_ep, opt)
             e1.record(stream)
             torch.cuda.synchronize()
             times.append(e0.elapsed_time(e1) / 1e3)
@@ -331,7 +333,7 @@ def main():
     # roofline of the dominant kernel (fused epoch kernel), events per launch
     st.reset(prob["init"])
     torch.cuda.synchronize()
-    k_ms, d_ms = st.run_profiled(0, n_ep)
+    k_ms, d_ms = st.run_profiled(0, n_ep, opt)
     avg_launch_s = k_ms / 1e3 / n_ep
     n_nodes = wl["n"]
     nd = 2
@@ -368,7 +370,7 @@ def main():
         e2e_steps = max(1, min(args.steps, 3))
         for _ in range(1):
             embd_p[...] = init
-            umapcu.optimise_embedding_adam_gpu(embd_p, A, prob["params"], prob["dens"], seed, 0, sampler)
+            umapcu.optimise_embedding_adam_gpu(embd_p, A, prob["params"], prob["dens"], seed, 0, sampler, opt)
         tt = []
         for _ in range(e2e_steps):
             embd_p[...] = init
@@ -376,7 +378,7 @@ def main():
             if dist:
                 dist.barrier()
             t0 = time.perf_counter()
-            umapcu.optimise_embedding_adam_gpu(embd_p, A, prob["params"], prob["dens"], seed, 0, sampler)
+            umapcu.optimise_embedding_adam_gpu(embd_p, A, prob["params"], prob["dens"], seed, 0, sampler, opt)
             tt.append(time.perf_counter() - t0)
         et = float(np.sum(tt))
         if dist:
@@ -397,7 +399,11 @@ def main():
         quality = {"trust15": q["trust"], "knn_preservation15": q["knn_preservation"], "queries": int(qn)}
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if args.optimiser == "sgd":
+        cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": "not timed: the reference's SGD (umap_optimisers.rs:653-865) is sequential over all "
+                         "edges; its parallel CPU path is the Adam one"}
+    elif rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         v, sample, secs = cpu_windows(prob, wl, seed, args.cpu_seconds, threads)
         cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
@@ -413,7 +419,7 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"{args.workload}: {wl['desc']}", "n_points": wl["n"], "n_edges": int(E),
                        "edge_updates_per_step": updates_per_step, "epochs": n_ep,
-                       "sampler": args.sampler, "l2": "flushed before every step (256 MiB write)",
+                       "sampler": args.sampler, "optimiser": args.optimiser, "l2": "flushed before every step (256 MiB write)",
                        "parallelism": f"replicas x{world}"},
             "roofline": roof,
             "cpu_baseline": cpu,

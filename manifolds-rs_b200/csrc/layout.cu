@@ -50,8 +50,13 @@ __global__ void __launch_bounds__(kWarps * 32, 6) k_epoch(const EpochArgs A)
 
 constexpr int kDensBlock = 256;
 
-// umap_dens_radii (umap_optimiser_gpu.rs:503-543) per node over every CSR
-// entry, plus a fixed-order f64 partial sum of the log radii per block.
+// umap_dens_radii (umap_optimiser_gpu.rs:503-543): per node, over its CSR
+// entries, sum phi and phi * d^2, then re = log(1e-8 + sum_sq / sum_phi).
+// Warp per 32-node segment (the block's 8 warps cover its 256 nodes): lanes
+// take consecutive CSR entries of the segment (coalesced `other` loads,
+// independent embedding gathers), and per-node sums come from a segmented
+// warp scan keyed by the entry's node, added to the node's lane. A
+// fixed-order f64 partial sum of the log radii per block follows.
 template <int D>
 __global__ void __launch_bounds__(kDensBlock) k_dens_radii(uint32_t n, const uint32_t *__restrict__ offsets,
                                                             const uint32_t *__restrict__ other,
@@ -60,39 +65,96 @@ __global__ void __launch_bounds__(kDensBlock) k_dens_radii(uint32_t n, const uin
                                                             float4 *__restrict__ dens_node,
                                                             double *__restrict__ part)
 {
-    __shared__ double sh[kDensBlock];
-    const uint32_t node = blockIdx.x * kDensBlock + threadIdx.x;
-    double rd = 0.0;
-    if (node < n) {
-        float ys[D], yo[D];
-        load_row<D>(y, node, ys);
-        float sum_sq = 0.0f, sum_phi = 0.0f;
-        for (uint32_t pos = offsets[node]; pos < offsets[node + 1]; pos++) {
-            load_row<D>(y, other[pos], yo);
+    constexpr int kW = kDensBlock / 32;
+    struct Seg {
+        uint32_t beg[33];
+        float ys[32][D];
+        float sums[32][2];
+    };
+    __shared__ Seg sm[kW];
+    __shared__ double shw[kW];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    Seg &S = sm[warp];
+    const uint32_t node0 = blockIdx.x * kDensBlock + warp * 32u;
+    const uint32_t node = node0 + lane;
+    const bool valid = node < n;
+    const uint32_t nc = min(node0, n);
+    S.beg[lane] = offsets[valid ? node : n];
+    if (lane == 31) S.beg[32] = offsets[min(nc + 32u, n)];
+    float ys[D];
+    if (valid) load_row<D>(y, node, ys);
+    else {
+#pragma unroll
+        for (int d = 0; d < D; d++) ys[d] = 0.0f;
+    }
+#pragma unroll
+    for (int d = 0; d < D; d++) S.ys[lane][d] = ys[d];
+    __syncwarp();
+    const uint32_t seg_beg = S.beg[0], seg_end = S.beg[32];
+    float sum_sq = 0.0f, sum_phi = 0.0f;
+    for (uint32_t c0 = seg_beg; c0 < seg_end; c0 += 32u) {
+        const uint32_t p = c0 + lane;
+        const bool live = p < seg_end;
+        uint32_t j = 32;
+        float t[2] = {0.0f, 0.0f};
+        if (live) {
+            j = local_node(S.beg, p);
+            float yo[D];
+            load_row<D>(y, other[p], yo);
             float dist_sq = 0.0f;
 #pragma unroll
             for (int d = 0; d < D; d++) {
-                float diff = ys[d] - yo[d];
+                float diff = S.ys[j][d] - yo[d];
                 dist_sq += diff * diff;
             }
             float dist_sq_b = pow_pos(dist_sq, b, precise);
             float phi = 1.0f / (1.0f + a * dist_sq_b);
-            sum_sq += phi * dist_sq;
-            sum_phi += phi;
+            t[0] = phi * dist_sq;
+            t[1] = phi;
         }
+        const uint32_t jprev = __shfl_up_sync(kFull, j, 1);
+        const uint32_t jnext = __shfl_down_sync(kFull, j, 1);
+        const unsigned heads = __ballot_sync(kFull, lane == 0 || jprev != j);
+        const int start = 31 - __clz(heads & (lane == 31 ? kFull : ((2u << lane) - 1u)));
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+#pragma unroll
+            for (int q = 0; q < 2; q++) {
+                const float v = __shfl_up_sync(kFull, t[q], off);
+                if (lane - off >= start) t[q] += v;
+            }
+        }
+        const bool tail = live && (lane == 31 || jnext != j);
+        if (tail) {
+            S.sums[j][0] = t[0];
+            S.sums[j][1] = t[1];
+        }
+        const unsigned has = __reduce_or_sync(kFull, tail ? (1u << j) : 0u);
+        __syncwarp();
+        if ((has >> lane) & 1u) {
+            sum_sq += S.sums[lane][0];
+            sum_phi += S.sums[lane][1];
+        }
+        __syncwarp();
+    }
+    double rd = 0.0;
+    if (valid) {
         float denom = sum_phi;
         if (denom < FLT_EPSILON) denom = FLT_EPSILON;
         float re = (float)log((double)(1e-8f + sum_sq / denom));
         dens_node[node] = make_float4(sum_phi, (float)exp((double)re), r[node], re);
         rd = (double)re;
     }
-    sh[threadIdx.x] = rd;
+    // fixed-order f64 sum: warp tree, then the block's warps in order
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) rd += __shfl_down_sync(kFull, rd, off);
+    if (lane == 0) shw[warp] = rd;
     __syncthreads();
-    for (int w = kDensBlock / 2; w > 0; w >>= 1) {
-        if ((int)threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
-        __syncthreads();
+    if (threadIdx.x == 0) {
+        double acc = 0.0;
+        for (int w = 0; w < kW; w++) acc += shw[w];
+        part[blockIdx.x] = acc;
     }
-    if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
 }
 
 // mean of the log radii from the per-block partials (fixed order)
