@@ -59,6 +59,7 @@ struct umapcu_batch {
     cudaStream_t s = nullptr;
     uint32_t n_probs = 0, n_dim = 0, n_epochs = 0, n_segs = 0;
     bool all_nr5 = true;
+    uint32_t sampler = UMAPCU_NEG_REF_HASH;
     std::vector<uint32_t> n;
     std::vector<DeviceCsr> csr;
     std::vector<DevBuf<float>> y0, y1, m, v, init;
@@ -123,9 +124,9 @@ void enqueue_run(umapcu_batch *b, const BatchConfig &c, uint32_t epochs, uint32_
     const uint32_t launches = c.mode == 1 ? 1 : epochs;
     for (uint32_t e = 0; e < launches; e++) {
         switch (b->n_dim) {
-            case 2: b->all_nr5 ? launch_batch_kernel<2>(B, c, s, e) : launch_batch_kernel_nr0<2>(B, c, s, e); break;
-            case 3: b->all_nr5 ? launch_batch_kernel<3>(B, c, s, e) : launch_batch_kernel_nr0<3>(B, c, s, e); break;
-            case 4: b->all_nr5 ? launch_batch_kernel<4>(B, c, s, e) : launch_batch_kernel_nr0<4>(B, c, s, e); break;
+            case 2: b->all_nr5 ? launch_batch_kernel<2>(B, c, s, e, b->sampler == UMAPCU_NEG_REF_HASH) : launch_batch_kernel_nr0<2>(B, c, s, e); break;
+            case 3: b->all_nr5 ? launch_batch_kernel<3>(B, c, s, e, b->sampler == UMAPCU_NEG_REF_HASH) : launch_batch_kernel_nr0<3>(B, c, s, e); break;
+            case 4: b->all_nr5 ? launch_batch_kernel<4>(B, c, s, e, b->sampler == UMAPCU_NEG_REF_HASH) : launch_batch_kernel_nr0<4>(B, c, s, e); break;
             default: fail(UMAPCU_BAD_ARG, "batched n_dim must be 2, 3 or 4");
         }
     }
@@ -235,6 +236,7 @@ umapcu_status umapcu_batch_create(uint32_t n_problems, const uint32_t *n, uint32
         cudaStream_t s = b->s;
         b->n_probs = n_problems;
         b->n_dim = n_dim;
+        b->sampler = sampler;
         b->n_epochs = n_epochs;
         b->n.assign(n, n + n_problems);
         b->csr.resize(n_problems);

@@ -74,7 +74,7 @@ __device__ __forceinline__ void epoch_args_of(const BatchProblem &P, uint32_t e,
     A.optimiser = optimiser;
 }
 
-template <int D, int NR, int KU>
+template <int D, int NR, int KU, bool FAST = false>
 __global__ void __launch_bounds__(kWarps * 32, 8) k_batch_persistent(const BatchArgs B)
 {
     __shared__ WarpSmem<D, KU> smem[kWarps];
@@ -112,7 +112,7 @@ __global__ void __launch_bounds__(kWarps * 32, 8) k_batch_persistent(const Batch
                 sargs[warp] = A;
             }
             __syncwarp();
-            epoch_segment<D, false, NR, true, KU>(sargs[warp], smem[warp], (s - P.seg_base) * 32u, lane);
+            epoch_segment<D, false, NR, true, KU, FAST>(sargs[warp], smem[warp], (s - P.seg_base) * 32u, lane);
         }
         __threadfence();
         __syncwarp();
@@ -120,7 +120,7 @@ __global__ void __launch_bounds__(kWarps * 32, 8) k_batch_persistent(const Batch
     }
 }
 
-template <int D, int NR, int KU>
+template <int D, int NR, int KU, bool FAST = false>
 __global__ void __launch_bounds__(kWarps * 32, 8) k_batch_epoch(const BatchArgs B, uint32_t e)
 {
     __shared__ WarpSmem<D, KU> smem[kWarps];
@@ -137,7 +137,7 @@ __global__ void __launch_bounds__(kWarps * 32, 8) k_batch_epoch(const BatchArgs 
         sargs[warp] = A;
     }
     __syncwarp();
-    epoch_segment<D, false, NR, false, KU>(sargs[warp], smem[warp], (s - P.seg_base) * 32u, lane);
+    epoch_segment<D, false, NR, false, KU, FAST>(sargs[warp], smem[warp], (s - P.seg_base) * 32u, lane);
 }
 
 struct BatchConfig {
@@ -146,19 +146,30 @@ struct BatchConfig {
     int ku = 8;          // scan super-chunk width
 };
 
-template <int D>
-inline void launch_batch_kernel(const BatchArgs &B, const BatchConfig &c, cudaStream_t s, uint32_t epoch)
+// fast: every problem uses the reference hash sampler (the batched and served
+// forms have no injected negatives and no precise mode), so the kernels can
+// take the compile-time fast path.
+template <int D, bool FAST>
+inline void launch_batch_kernel_t(const BatchArgs &B, const BatchConfig &c, cudaStream_t s, uint32_t epoch)
 {
     if (c.mode == 1) {
         const unsigned grid = (unsigned)(c.ctas_per_sm * device_sm_count());
-        if (c.ku == 4) k_batch_persistent<D, 5, 4><<<grid, kWarps * 32, 0, s>>>(B);
-        else k_batch_persistent<D, 5, 8><<<grid, kWarps * 32, 0, s>>>(B);
+        if (c.ku == 4) k_batch_persistent<D, 5, 4, FAST><<<grid, kWarps * 32, 0, s>>>(B);
+        else k_batch_persistent<D, 5, 8, FAST><<<grid, kWarps * 32, 0, s>>>(B);
     } else {
         const unsigned grid = ceil_div(B.n_segs, kWarps);
-        if (c.ku == 4) k_batch_epoch<D, 5, 4><<<grid, kWarps * 32, 0, s>>>(B, epoch);
-        else k_batch_epoch<D, 5, 8><<<grid, kWarps * 32, 0, s>>>(B, epoch);
+        if (c.ku == 4) k_batch_epoch<D, 5, 4, FAST><<<grid, kWarps * 32, 0, s>>>(B, epoch);
+        else k_batch_epoch<D, 5, 8, FAST><<<grid, kWarps * 32, 0, s>>>(B, epoch);
     }
     check_launch("k_batch");
+}
+
+template <int D>
+inline void launch_batch_kernel(const BatchArgs &B, const BatchConfig &c, cudaStream_t s, uint32_t epoch,
+                                bool fast)
+{
+    if (fast) launch_batch_kernel_t<D, true>(B, c, s, epoch);
+    else launch_batch_kernel_t<D, false>(B, c, s, epoch);
 }
 
 template <int D>

@@ -344,7 +344,7 @@ void umapcu_server::tick_launch()
 {
     hp.assign(active.size(), BatchProblem{});
     segs.clear();
-    bool nr5 = true;
+    bool nr5 = true, all_hash = true;
     for (size_t i = 0; i < active.size(); i++) {
         ServeJob *j = active[i];
         BatchProblem &P = hp[i];
@@ -373,6 +373,7 @@ void umapcu_server::tick_launch()
         P.omb2 = 1.0f - q.beta2;
         P.neg_rate = q.neg_sample_rate;
         nr5 = nr5 && q.neg_sample_rate == 5;
+        all_hash = all_hash && j->sampler == UMAPCU_NEG_REF_HASH;
         P.sampler = j->sampler;
         P.seed32 = (uint32_t)j->seed;
         P.seed_lo = (uint32_t)j->seed;
@@ -402,9 +403,9 @@ void umapcu_server::tick_launch()
     c.mode = 1;
     c.ctas_per_sm = tick_ctas;
     switch (n_dim) {
-        case 2: nr5 ? launch_batch_kernel<2>(B, c, s, 0) : launch_batch_kernel_nr0<2>(B, c, s, 0); break;
-        case 3: nr5 ? launch_batch_kernel<3>(B, c, s, 0) : launch_batch_kernel_nr0<3>(B, c, s, 0); break;
-        default: nr5 ? launch_batch_kernel<4>(B, c, s, 0) : launch_batch_kernel_nr0<4>(B, c, s, 0); break;
+        case 2: nr5 ? launch_batch_kernel<2>(B, c, s, 0, all_hash) : launch_batch_kernel_nr0<2>(B, c, s, 0); break;
+        case 3: nr5 ? launch_batch_kernel<3>(B, c, s, 0, all_hash) : launch_batch_kernel_nr0<3>(B, c, s, 0); break;
+        default: nr5 ? launch_batch_kernel<4>(B, c, s, 0, all_hash) : launch_batch_kernel_nr0<4>(B, c, s, 0); break;
     }
     d2h(&err_h, ctr.p + 1, 1, s);
 }
