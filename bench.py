@@ -548,20 +548,23 @@ def run_served(args, wl, world, rank, local_rank):
         g = int(req_graph[r])
         return umapcu.random_layout(pool[g].n, 2, seed + 9000 + r)
 
-    # capacity: the server's own throughput under a saturating burst (every
-    # request submitted at once; admission, graph builds and ticks included),
-    # embeddings/s for this size mix
-    n_cal = 4 * len(pool)
+    # capacity: the server's own steady-state throughput under a saturating
+    # burst (every request submitted at once; admission, graph builds and
+    # ticks included), embeddings/s for this size mix, taken between the
+    # 10th and 90th percentile completions (ramp-up and drain excluded)
+    n_cal = 20 * len(pool)
     cal_rng = np.random.default_rng(seed + 5)
     cal = [(pool[int(g)], umapcu.random_layout(pool[int(g)].n, 2, seed + 7000 + i))
            for i, g in enumerate(cal_rng.integers(0, len(pool), n_cal))]
     sv = umapcu.UmapServer(budget_bytes=wl["budget"], max_jobs=4096, tick_epochs=10, n_dim=2)
     for g, y0 in cal[:len(pool)]:  # warm-up
         sv.wait(sv.submit(y0, g, params, seed=1))
-    tb = time.perf_counter()
-    for t in [sv.submit(y0, g, params, seed=i) for i, (g, y0) in enumerate(cal)]:
-        sv.wait(t)
-    cap = n_cal / (time.perf_counter() - tb)
+    subs = []
+    for i, (g, y0) in enumerate(cal):
+        subs.append((time.perf_counter(), sv.submit(y0, g, params, seed=i)))
+    done = np.sort([t0 + sv.wait(t)[1] for t0, t in subs])
+    lo, hi = int(0.1 * n_cal), int(0.9 * n_cal)
+    cap = (hi - lo) / (done[hi] - done[lo])
     sv.close()
     lam = wl["util"] * cap
     gaps = rng.exponential(1.0 / lam, n_req)
