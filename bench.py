@@ -307,10 +307,10 @@ def main():
         st.run(0, n_ep, opt)
     torch.cuda.synchronize()
 
-    times = []
-    with ClockSampler(local_rank) as clk:
+    def time_steps(state):
+        out = []
         for _ in range(args.steps):
-            st.reset(prob["init"])
+            state.reset(prob["init"])
             flush.fill_(1.0)
             torch.cuda.synchronize()
             if dist:
@@ -318,10 +318,31 @@ def main():
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            st.run(0, n_ep, opt)
+            state.run(0, n_ep, opt)
             e1.record(stream)
             torch.cuda.synchronize()
-            times.append(e0.elapsed_time(e1) / 1e3)
+            out.append(e0.elapsed_time(e1) / 1e3)
+        return out
+
+    with ClockSampler(local_rank) as clk:
+        times = time_steps(st)
+    sched = st.schedule_info()
+    scan_value = None
+    if sched["lists"]:
+        # the same steps on a state that scans the CSR every epoch
+        os.environ["UMAPCU_NO_SCHEDULE_LISTS"] = "1"
+        st2 = umapcu.UmapGpuState(prob["init"], prob["adj"], prob["params"], prob["dens"], seed, sampler)
+        del os.environ["UMAPCU_NO_SCHEDULE_LISTS"]
+        st2.set_stream(stream.cuda_stream)
+        st2.reset(prob["init"])
+        st2.run(0, n_ep, opt)
+        t2 = float(np.sum(time_steps(st2)))
+        if dist:
+            tt = torch.tensor([t2], device="cuda", dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t2 = float(tt.item())
+        scan_value = world * args.steps * updates_per_step / t2
+        st2.close()
     total = float(np.sum(times))
     if dist:
         t = torch.tensor([total], device="cuda", dtype=torch.float64)
@@ -419,7 +440,12 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"{args.workload}: {wl['desc']}", "n_points": wl["n"], "n_edges": int(E),
                        "edge_updates_per_step": updates_per_step, "epochs": n_ep,
-                       "sampler": args.sampler, "optimiser": args.optimiser, "l2": "flushed before every step (256 MiB write)",
+                       "sampler": args.sampler, "optimiser": args.optimiser,
+                       "schedule": ("per-epoch active-entry lists built at state creation "
+                                    f"({sched['build_ms']:.1f} ms, {sched['records']} records; outside the timed "
+                                    "region like the CSR build)") if sched["lists"] else "CSR scan every epoch",
+                       "value_csr_scan": scan_value,
+                       "l2": "flushed before every step (256 MiB write)",
                        "parallelism": f"replicas x{world}"},
             "roofline": roof,
             "cpu_baseline": cpu,

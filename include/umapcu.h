@@ -351,6 +351,18 @@ umapcu_status umapcu_sample_negatives(uint32_t sampler, uint64_t seed, uint32_t 
                                       uint32_t entry, uint32_t epoch, uint32_t edge_local,
                                       uint32_t count, uint32_t n, uint32_t *out);
 
+/* Schedule lists of a state (no reference counterpart): a state made by
+ * umapcu_state_create precomputes, for every epoch of params.n_epochs, the
+ * CSR entries the edge schedule (umap_optimiser_gpu.rs:940-955) activates
+ * (the same f32 cursor arithmetic), so its epochs read those records instead
+ * of scanning every entry's cursor. Results are bit-identical to the scan;
+ * runs that skip or repeat epochs fall back to the scan until
+ * umapcu_state_reset. Set UMAPCU_NO_SCHEDULE_LISTS to disable; the one-shot
+ * umapcu_optimise_embedding always scans. lists_active: 1 when built;
+ * n_records: records held (8 bytes each); build_ms: build time. */
+umapcu_status umapcu_state_schedule_info(const umapcu_state *st, int *lists_active, uint64_t *n_records,
+                                         float *build_ms);
+
 /* ------------------------------------------------ kNN, metrics, kNN cache */
 
 /* Distance metrics of the neighbour search (NearestNeighbourParams::

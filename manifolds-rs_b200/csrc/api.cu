@@ -41,6 +41,13 @@ struct umapcu_state {
     DevBuf<double> part1, mean;
     DevBuf<double2> part2;
     DevBuf<float> stats;
+    // schedule lists (schedule.cu): usable while the epochs run so far are
+    // 0, 1, ..., sched_epoch - 1 from the reset schedule; the cursors in
+    // csr.sched then lag (sched_lazy) until something needs them
+    ScheduleLists lists;
+    bool lists_ok = false, sched_continuous = true, sched_lazy = false;
+    uint32_t sched_epoch = 0;
+    float lists_build_ms = 0.0f;
 };
 
 namespace {
@@ -96,12 +103,30 @@ void dens_update(umapcu_state *st)
     launch_dens_update(D, st->n_dim, st->stream.s);
 }
 
+// Cursors in csr.sched brought up to date (after list-mode epochs).
+void sync_cursors(umapcu_state *st)
+{
+    if (!st->sched_lazy) return;
+    materialise_schedule(st->csr, st->sched_epoch, st->stream.s);
+    st->sched_lazy = false;
+}
+
 void run_epoch(umapcu_state *st, uint32_t epoch, uint32_t optimiser, const uint32_t *d_inj, float *d_grad,
                uint32_t *d_act, bool skip_dens = false)
 {
     const bool dens_on = st->dens && dens_active(st->lambda, st->frac, epoch, st->p.n_epochs);
     if (dens_on && !skip_dens) dens_update(st);
+    const bool in_order = st->sched_continuous && epoch == st->sched_epoch;
+    const bool use_lists = st->lists_ok && in_order && epoch < st->lists.n_epochs;
+    if (!use_lists) sync_cursors(st);  // the scan reads and advances the cursors
+    if (!in_order) st->sched_continuous = false;
     EpochArgs A{};
+    if (use_lists) {
+        A.rec = st->lists.rec.p;
+        A.seg_ptr = st->lists.seg_ptr.p + (size_t)epoch * st->lists.nseg;
+        st->sched_lazy = true;
+    }
+    if (in_order) st->sched_epoch = epoch + 1;
     A.n = st->n;
     A.offsets = st->csr.offsets.p;
     A.other = st->csr.other.p;
@@ -157,7 +182,7 @@ struct PhaseTimer {
 umapcu_status create_state(const float *embd, uint32_t n, uint32_t n_dim, const uint64_t *adj_ptr,
                            const uint32_t *adj_col, const float *adj_w, const umapcu_optim_params *params,
                            const umapcu_dens *dens, uint64_t seed, uint32_t sampler,
-                           std::unique_ptr<umapcu_state> &out)
+                           std::unique_ptr<umapcu_state> &out, bool lists)
 {
     if (n == 0) return UMAPCU_NO_DATA;
     if (!embd || !adj_ptr) return UMAPCU_BAD_ARG;
@@ -187,6 +212,17 @@ umapcu_status create_state(const float *embd, uint32_t n, uint32_t n_dim, const 
         umapcu_status rc = build_csr_dev(n, dptr.p, dcol.p, dw.p, nnz, st->csr, s);
         if (rc != UMAPCU_OK) return rc;
         T.mark("CSR build", s);
+    }
+    // Schedule lists pay for their build (a few ms at 1M points) over repeated
+    // or resumed runs of a resident state; a one-shot call scans instead.
+    if (lists && !getenv("UMAPCU_NO_SCHEDULE_LISTS")) {
+        sync(s);
+        const auto t0 = std::chrono::steady_clock::now();
+        st->lists_ok = build_schedule_lists(st->csr, params->n_epochs, st->lists, s);
+        sync(s);
+        st->lists_build_ms =
+            (float)std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        T.mark("schedule lists", s);
     }
     const uint64_t nt = (uint64_t)n * n_dim;
     st->y[0].alloc(nt, s);
@@ -413,7 +449,7 @@ umapcu_status umapcu_state_create(const float *embd, uint32_t n, uint32_t n_dim,
         if (!out) return UMAPCU_BAD_ARG;
         *out = nullptr;
         std::unique_ptr<umapcu_state> st;
-        umapcu_status rc = create_state(embd, n, n_dim, adj_ptr, adj_col, adj_w, params, dens, seed, sampler, st);
+        umapcu_status rc = create_state(embd, n, n_dim, adj_ptr, adj_col, adj_w, params, dens, seed, sampler, st, true);
         if (rc == UMAPCU_OK) *out = st.release();
         return rc;
     });
@@ -426,6 +462,16 @@ umapcu_status umapcu_state_sizes(const umapcu_state *st, uint64_t *n, uint64_t *
     if (!st) return UMAPCU_BAD_ARG;
     if (n) *n = st->n;
     if (n_edges) *n_edges = st->csr.n_edges;
+    return UMAPCU_OK;
+}
+
+umapcu_status umapcu_state_schedule_info(const umapcu_state *st, int *lists_active, uint64_t *n_records,
+                                         float *build_ms)
+{
+    if (!st) return UMAPCU_BAD_ARG;
+    if (lists_active) *lists_active = st->lists_ok ? 1 : 0;
+    if (n_records) *n_records = st->lists.n_records;
+    if (build_ms) *build_ms = st->lists_build_ms;
     return UMAPCU_OK;
 }
 
@@ -491,6 +537,7 @@ umapcu_status umapcu_state_read(const umapcu_state *st, float *embd, float *m, f
         if (m) d2h(m, st->m.p, nt, s);
         if (v) d2h(v, st->v.p, nt, s);
         if (cursor) {
+            sync_cursors(const_cast<umapcu_state *>(st));
             DevBuf<float> c(st->csr.n_edges, s);
             k_edge_cursor<<<ceil_div(st->n, 256), 256, 0, s>>>(st->n, st->csr.offsets.p, st->csr.other.p,
                                                                st->csr.edge_id.p, st->csr.sched.p, c.p);
@@ -527,6 +574,9 @@ umapcu_status umapcu_state_reset(umapcu_state *st, const float *embd)
         check_cuda(cudaMemsetAsync(st->m.p, 0, nt * sizeof(float), s), "memset m");
         check_cuda(cudaMemsetAsync(st->v.p, 0, nt * sizeof(float), s), "memset v");
         reset_schedule_dev(st->csr, s);
+        st->sched_epoch = 0;
+        st->sched_continuous = true;
+        st->sched_lazy = false;
         sync(s);
         return UMAPCU_OK;
     });
@@ -628,7 +678,7 @@ umapcu_status umapcu_optimise_embedding(float *embd, uint32_t n, uint32_t n_dim,
     return guard([&]() -> umapcu_status {
         if (optimiser > UMAPCU_OPT_SGD) return UMAPCU_BAD_ARG;
         std::unique_ptr<umapcu_state> st;
-        umapcu_status rc = create_state(embd, n, n_dim, adj_ptr, adj_col, adj_w, params, dens, seed, sampler, st);
+        umapcu_status rc = create_state(embd, n, n_dim, adj_ptr, adj_col, adj_w, params, dens, seed, sampler, st, false);
         if (rc != UMAPCU_OK) return rc;
         if (verbose)
             printf("Running %u epochs with GPU-accelerated %s optimisation.\n", params->n_epochs,

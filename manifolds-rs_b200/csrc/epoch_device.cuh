@@ -366,7 +366,9 @@ __device__ __forceinline__ void process_batch(const EpochArgs &A, WarpSmem<D, KU
 
 // One epoch of one 32-node segment [node0, node0 + 32) of problem A, run by
 // one warp (see the file comment).
-template <int D, bool DENS, int NR, bool COH, int KU = kU, bool FAST = false>
+// LIST: the segment's active entries come from the epoch's schedule lists
+// (A.rec / A.seg_ptr) instead of a scan of its CSR range.
+template <int D, bool DENS, int NR, bool COH, int KU = kU, bool FAST = false, bool LIST = false>
 __device__ __forceinline__ void epoch_segment(const EpochArgs &A, WarpSmem<D, KU> &S, uint32_t node0, int lane)
 {
     __syncwarp();  // the warp's shared memory may still be read by its previous segment
@@ -393,6 +395,22 @@ __device__ __forceinline__ void epoch_segment(const EpochArgs &A, WarpSmem<D, KU
     for (int d = 0; d < D; d++) g[d] = 0.0f;
     bool act = false;
     __syncwarp();
+    if constexpr (LIST) {
+        // records in CSR order, 32 per batch; the next chunk's records are
+        // loaded while the current batch runs
+        const uint32_t sg = node0 >> 5;
+        const uint64_t r0 = A.seg_ptr[sg], r1 = A.seg_ptr[sg + 1];
+        uint2 nx = make_uint2(0, 0);
+        if (r0 + lane < r1) nx = __ldcs(A.rec + r0 + lane);
+        for (uint64_t q = r0; q < r1; q += 32) {
+            const uint32_t cnt = (uint32_t)min((uint64_t)32, r1 - q);
+            S.qp[lane] = nx.x;
+            S.qo[lane] = nx.y;
+            if (q + 32 + lane < r1) nx = __ldcs(A.rec + q + 32 + lane);
+            __syncwarp();
+            process_batch<D, DENS, NR, COH, KU, FAST>(A, S, 0, cnt, node0, lane, g, act, dstat);
+        }
+    } else {
     const uint32_t seg_beg = S.beg[0], seg_end = S.beg[32];
     const unsigned lt_mask = (1u << lane) - 1u;
     uint32_t count = 0;
@@ -441,6 +459,7 @@ __device__ __forceinline__ void epoch_segment(const EpochArgs &A, WarpSmem<D, KU
             __syncwarp();
         }
         count = rem;
+    }
     }
     if (!valid) return;
     float yn[D];

@@ -196,6 +196,22 @@ void knn_dev(const float *d_x, uint32_t n, uint32_t dim, const uint32_t *d_qidx,
 void knn_rank_dev(const float *d_x, uint32_t n, uint32_t dim, const uint32_t *d_qidx, uint32_t nq,
                   const uint32_t *d_nbr, uint32_t k, uint32_t metric, uint32_t *d_counts, cudaStream_t s);
 
+// Per-epoch lists of active CSR entries (schedule.cu): rec [n_records]
+// (CSR position, other endpoint), seg_ptr [n_epochs * nseg + 1].
+struct ScheduleLists {
+    DevBuf<uint2> rec;
+    DevBuf<uint64_t> seg_ptr;
+    uint64_t n_records = 0;
+    uint32_t n_epochs = 0, nseg = 0;
+};
+// Builds the lists for epochs [0, n_epochs) from the reset schedule (cursor
+// = period); false when they would not fit (half the free device memory) or
+// n_epochs is out of range, `out` then empty.
+bool build_schedule_lists(const DeviceCsr &csr, uint32_t n_epochs, ScheduleLists &out, cudaStream_t s);
+// Writes into csr.sched the cursors after `epochs` epochs from the reset
+// schedule (the state the per-epoch scan would have left).
+void materialise_schedule(DeviceCsr &csr, uint32_t epochs, cudaStream_t s);
+
 // Resets every entry's schedule cursor to its period (upload state,
 // umap_optimiser_gpu.rs:425-430).
 void reset_schedule_dev(DeviceCsr &csr, cudaStream_t s);

@@ -36,14 +36,14 @@
 
 namespace umapcu {
 
-template <int D, bool DENS, int NR, bool FAST = false>
+template <int D, bool DENS, int NR, bool FAST = false, bool LIST = false>
 __global__ void __launch_bounds__(kWarps * 32, 6) k_epoch(const EpochArgs A)
 {
     __shared__ WarpSmem<D> smem[kWarps];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t node0 = (blockIdx.x * kWarps + warp) * 32u;
     if (node0 >= A.n) return;
-    epoch_segment<D, DENS, NR, false, kU, FAST>(A, smem[warp], node0, lane);
+    epoch_segment<D, DENS, NR, false, kU, FAST, LIST>(A, smem[warp], node0, lane);
 }
 
 // ------------------------------------------------------------ densMAP
@@ -252,9 +252,16 @@ static void launch_epoch_t(const EpochArgs &A, cudaStream_t s)
 {
     const uint32_t nseg = ceil_div(A.n, 32);
     const bool fast = !A.injected && A.sampler == UMAPCU_NEG_REF_HASH && !A.precise_pow;
-    if (A.neg_rate == 5 && fast) k_epoch<D, DENS, 5, true><<<ceil_div(nseg, kWarps), kWarps * 32, 0, s>>>(A);
-    else if (A.neg_rate == 5) k_epoch<D, DENS, 5><<<ceil_div(nseg, kWarps), kWarps * 32, 0, s>>>(A);
-    else k_epoch<D, DENS, 0><<<ceil_div(nseg, kWarps), kWarps * 32, 0, s>>>(A);
+    const unsigned grid = ceil_div(nseg, kWarps);
+    if (A.rec) {
+        if (A.neg_rate == 5 && fast) k_epoch<D, DENS, 5, true, true><<<grid, kWarps * 32, 0, s>>>(A);
+        else if (A.neg_rate == 5) k_epoch<D, DENS, 5, false, true><<<grid, kWarps * 32, 0, s>>>(A);
+        else k_epoch<D, DENS, 0, false, true><<<grid, kWarps * 32, 0, s>>>(A);
+    } else {
+        if (A.neg_rate == 5 && fast) k_epoch<D, DENS, 5, true><<<grid, kWarps * 32, 0, s>>>(A);
+        else if (A.neg_rate == 5) k_epoch<D, DENS, 5><<<grid, kWarps * 32, 0, s>>>(A);
+        else k_epoch<D, DENS, 0><<<grid, kWarps * 32, 0, s>>>(A);
+    }
 }
 
 void launch_epoch(const EpochArgs &A, uint32_t n_dim, bool dens, cudaStream_t s)

@@ -143,6 +143,7 @@ _SIGS = {
     "umapcu_server_stats": [_vp, _vp, _vp, _vp, _vp],
     "umapcu_eval_pow": [_vp, _u32, _f32, _i32, _vp],
     "umapcu_knn_exact": [_vp, _u32, _u32, _u32, _u32, _vp, _vp],
+    "umapcu_state_schedule_info": [_vp, _vp, _vp, _vp],
     "umapcu_knn_exact_dev": [_vp, _u32, _u32, _vp, _u32, _u32, _u32, _vp, _vp, _vp],
     "umapcu_embedding_quality": [_vp, _u32, _u32, _vp, _u32, _vp, _u32, _u32, _vp, _u32, _u32, _vp, _vp],
     "umapcu_fuzzy_cross_entropy": [_vp, _vp, _vp, _u64, _vp, _u32, _u32, _f32, _f32, _vp],
@@ -429,6 +430,13 @@ class UmapGpuState:
         mu = np.empty(E, np.float32)
         _check(_lib.umapcu_state_read_csr(self._h, _p(off), _p(ei), _p(ot), _p(eps), _p(mu)))
         return dict(n=self.n, n_edges=E, offsets=off, edge_idx=ei, other=ot, eps=eps, mu=mu)
+
+    def schedule_info(self):
+        """-> dict(lists=bool, records=int, build_ms=float): the state's
+        per-epoch active-entry lists (see umapcu_state_schedule_info)."""
+        a, r, ms = C.c_int(), C.c_uint64(), C.c_float()
+        _check(_lib.umapcu_state_schedule_info(self._h, C.byref(a), C.byref(r), C.byref(ms)))
+        return dict(lists=bool(a.value), records=r.value, build_ms=ms.value)
 
     def run(self, first_epoch: int, count: int, optimiser: int = OPT_ADAM):
         _check(_lib.umapcu_state_run(self._h, first_epoch, count, optimiser))

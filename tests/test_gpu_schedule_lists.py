@@ -1,0 +1,81 @@
+"""Schedule lists (per-epoch active-entry records built once per state) vs
+the per-epoch CSR scan: the same active entries in the same CSR order and
+batch boundaries, so results must agree bit for bit, for in-order runs, for
+runs that skip epochs (the state falls back to the scan), after reset, and
+with the densMAP term (needs a B200)."""
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+umapcu = pytest.importorskip("umapcu")
+from tests._problems import init_embedding, oracle_graph
+
+
+def _state(adj, emb, p, lists, dens=None, seed=9):
+    old = os.environ.pop("UMAPCU_NO_SCHEDULE_LISTS", None)
+    try:
+        if not lists:
+            os.environ["UMAPCU_NO_SCHEDULE_LISTS"] = "1"
+        return umapcu.UmapGpuState(emb, adj, p, dens, seed)
+    finally:
+        os.environ.pop("UMAPCU_NO_SCHEDULE_LISTS", None)
+        if old is not None:
+            os.environ["UMAPCU_NO_SCHEDULE_LISTS"] = old
+
+
+@pytest.fixture(scope="module")
+def prob():
+    g = oracle_graph(n=3000, dim=50, k=15, n_epochs=80)
+    return g, umapcu.Adjacency(g["ptr"], g["col"], g["val"])
+
+
+@pytest.mark.parametrize("calls", [[(0, 80)], [(0, 30), (30, 50)], [(0, 10), (20, 5), (25, 40)],
+                                   [(0, 40), (40, 60)]])
+def test_lists_equal_scan(prob, calls):
+    g, adj = prob
+    p = umapcu.UmapOptimParams(n_epochs=80)
+    emb = init_embedding(3000, 2, seed=4)
+    a, b = _state(adj, emb, p, True), _state(adj, emb, p, False)
+    for first, count in calls:  # (40, 60) runs past the lists' 80 epochs
+        a.run(first, count)
+        b.run(first, count)
+        ya, ma, va, ca = a.read()
+        yb, mb, vb, cb = b.read()
+        assert np.array_equal(ya, yb) and np.array_equal(ma, mb) and np.array_equal(va, vb)
+        assert np.array_equal(ca, cb)  # cursors materialised from the lists
+    a.reset(emb)
+    b.reset(emb)
+    a.run(0, 80)
+    b.run(0, 80)
+    assert np.array_equal(a.read()[0], b.read()[0])
+    a.close()
+    b.close()
+
+
+def test_lists_equal_scan_sgd_and_debug_epochs(prob):
+    g, adj = prob
+    p = umapcu.UmapOptimParams(n_epochs=50)
+    emb = init_embedding(3000, 2, seed=6)
+    a, b = _state(adj, emb, p, True), _state(adj, emb, p, False)
+    a.run(0, 20, umapcu.OPT_SGD)
+    b.run(0, 20, umapcu.OPT_SGD)
+    ga, ha = a.epoch_debug(20)
+    gb, hb = b.epoch_debug(20)
+    assert np.array_equal(ga, gb) and np.array_equal(ha, hb)
+    assert np.array_equal(a.read()[0], b.read()[0])
+
+
+def test_lists_equal_scan_densmap():
+    g = oracle_graph(n=2500, dim=30, k=15, n_epochs=60)
+    coo = umapcu.CoordinateList(g["row"], g["col"], g["val"], 2500)
+    dens = umapcu.DensState.new(umapcu.DensParams(), coo, g["idx"], g["dist"], True)
+    adj = umapcu.Adjacency(g["ptr"], g["col"], g["val"])
+    p = umapcu.UmapOptimParams(n_epochs=60)
+    emb = init_embedding(2500, 2, seed=8)
+    a, b = _state(adj, emb, p, True, dens), _state(adj, emb, p, False, dens)
+    a.run(0, 60)
+    b.run(0, 60)
+    assert np.array_equal(a.read()[0], b.read()[0])
