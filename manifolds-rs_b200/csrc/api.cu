@@ -123,7 +123,8 @@ void run_epoch(umapcu_state *st, uint32_t epoch, uint32_t optimiser, const uint3
     EpochArgs A{};
     if (use_lists) {
         A.rec = st->lists.rec.p;
-        A.seg_ptr = st->lists.seg_ptr.p + (size_t)epoch * st->lists.nseg;
+        A.seg_ptr = st->lists.ptr.p + (size_t)epoch * st->lists.n_units;
+        A.seg_unit = st->lists.unit_base.p;
         st->sched_lazy = true;
     }
     if (in_order) st->sched_epoch = epoch + 1;

@@ -399,7 +399,7 @@ __device__ __forceinline__ void epoch_segment(const EpochArgs &A, WarpSmem<D, KU
         // records in CSR order, 32 per batch; the next chunk's records are
         // loaded while the current batch runs
         const uint32_t sg = node0 >> 5;
-        const uint64_t r0 = A.seg_ptr[sg], r1 = A.seg_ptr[sg + 1];
+        const uint64_t r0 = A.seg_ptr[A.seg_unit[sg]], r1 = A.seg_ptr[A.seg_unit[sg + 1]];
         uint2 nx = make_uint2(0, 0);
         if (r0 + lane < r1) nx = __ldcs(A.rec + r0 + lane);
         for (uint64_t q = r0; q < r1; q += 32) {

@@ -197,12 +197,15 @@ void knn_rank_dev(const float *d_x, uint32_t n, uint32_t dim, const uint32_t *d_
                   const uint32_t *d_nbr, uint32_t k, uint32_t metric, uint32_t *d_counts, cudaStream_t s);
 
 // Per-epoch lists of active CSR entries (schedule.cu): rec [n_records]
-// (CSR position, other endpoint), seg_ptr [n_epochs * nseg + 1].
+// (CSR position, other endpoint); ptr [n_epochs * n_units + 1] record
+// offsets per (epoch, work unit); unit_base [nseg + 1] each segment's first
+// work unit.
 struct ScheduleLists {
     DevBuf<uint2> rec;
-    DevBuf<uint64_t> seg_ptr;
+    DevBuf<uint64_t> ptr;
+    DevBuf<uint32_t> unit_base;
     uint64_t n_records = 0;
-    uint32_t n_epochs = 0, nseg = 0;
+    uint32_t n_epochs = 0, nseg = 0, n_units = 0;
 };
 // Builds the lists for epochs [0, n_epochs) from the reset schedule (cursor
 // = period); false when they would not fit (half the free device memory) or

@@ -20,7 +20,8 @@ struct EpochArgs {
     const float4 *dens_node;   // [n] {phi_sum, exp(re), r, re} (densMAP only)
     const float *dens_stats;   // {mean, std, cov, inv_var, coeff} (densMAP only)
     const uint2 *rec;          // schedule lists: (CSR position, other) of active entries, or nullptr (scan)
-    const uint64_t *seg_ptr;   // schedule lists: [nseg + 1] record offsets of this epoch's segments
+    const uint64_t *seg_ptr;   // schedule lists: this epoch's record offsets per work unit
+    const uint32_t *seg_unit;  // schedule lists: [nseg + 1] each segment's first work unit
     const uint32_t *injected;  // [2E * neg_rate] injected negatives or nullptr
     float *dbg_grad;           // [n * D] gradient output or nullptr
     uint32_t *dbg_active;      // [n] has_update output or nullptr

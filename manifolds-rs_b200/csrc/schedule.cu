@@ -11,9 +11,11 @@
 // (cursor, period) and other endpoint each epoch.
 //
 // Layout: rec [R] = (CSR position, other endpoint) of the active entries,
-// epoch-major, then segment, then CSR order; seg_ptr [n_epochs * nseg + 1] = exclusive scan of
-// the per-(epoch, segment) counts, so epoch e, segment s owns
-// rec[seg_ptr[e * nseg + s] .. seg_ptr[e * nseg + s + 1]).
+// epoch-major, then work unit (units of a segment adjacent), then CSR order;
+// ptr [n_epochs * n_units + 1] = exclusive scan of the per-(epoch, unit)
+// counts and unit_base [nseg + 1] the segments' first units, so epoch e,
+// segment s owns rec[ptr[e * n_units + unit_base[s]] ..
+// ptr[e * n_units + unit_base[s + 1]]).
 #include <chrono>
 #include <cstdlib>
 
@@ -25,89 +27,74 @@ namespace umapcu {
 namespace {
 
 constexpr int kSchedWarps = 4;
-// Segments with at most this many CSR entries keep their cursors in shared
-// memory and are walked epoch by epoch (each (epoch, segment) cell written
-// contiguously by one warp); longer ones walk chunk by chunk.
+// A work unit is at most kSchedCap consecutive CSR entries of one segment
+// (a segment of L entries has ceil(L / kSchedCap) units, at least one): one
+// warp per unit keeps the unit's cursors in shared memory and walks epoch by
+// epoch, so a hub-heavy segment does not hold one warp for its whole length.
 constexpr uint32_t kSchedCap = 1024;
 
-// One warp per segment. counts [n_epochs][nseg] (pass 1) or, with rec
-// non-null, the records written at seg_ptr (pass 2).
+__global__ void k_sched_units(const uint32_t *__restrict__ offsets, uint32_t n, uint32_t nseg,
+                              uint32_t *__restrict__ units)
+{
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nseg) return;
+    const uint32_t len = offsets[min(s * 32u + 32u, n)] - offsets[s * 32u];
+    units[s] = len ? (len + kSchedCap - 1) / kSchedCap : 1u;
+}
+
+// One warp per unit. counts [n_epochs][n_units] (pass 1) or, with rec
+// non-null, the records written from ptr (pass 2).
 __global__ void __launch_bounds__(kSchedWarps * 32) k_sched_lists(const uint32_t *__restrict__ offsets,
                                                                   const uint32_t *__restrict__ other,
                                                                   const float2 *__restrict__ sched, uint32_t n,
-                                                                  uint32_t nseg, uint32_t n_epochs,
+                                                                  uint32_t nseg, const uint32_t *__restrict__ unit_base,
+                                                                  uint32_t n_units, uint32_t n_epochs,
                                                                   uint32_t *__restrict__ counts,
-                                                                  const uint64_t *__restrict__ seg_ptr,
+                                                                  const uint64_t *__restrict__ ptr,
                                                                   uint2 *__restrict__ rec)
 {
     extern __shared__ float2 cur[];  // [kSchedWarps][kSchedCap] (cursor, period)
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t s = blockIdx.x * kSchedWarps + warp;
-    if (s >= nseg) return;  // warp-uniform
-    float2 *my = cur + (size_t)warp * kSchedCap;
-    const uint32_t beg = offsets[s * 32u], end = offsets[min(s * 32u + 32u, n)];
+    const uint32_t u = blockIdx.x * kSchedWarps + warp;
+    if (u >= n_units) return;  // warp-uniform
+    // the unit's segment: largest s with unit_base[s] <= u
+    uint32_t lo = 0, hi = nseg;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (unit_base[mid] <= u) lo = mid;
+        else hi = mid;
+    }
+    const uint32_t s = lo, piece = u - unit_base[s];
+    const uint32_t sbeg = offsets[s * 32u], send = offsets[min(s * 32u + 32u, n)];
+    const uint32_t beg = min(send, sbeg + piece * kSchedCap), end = min(send, beg + kSchedCap);
     const uint32_t len = end - beg;
+    float2 *my = cur + (size_t)warp * kSchedCap;
     const unsigned lt = (1u << lane) - 1u;
-    if (len <= kSchedCap) {
-        // epoch-major: cursors in shared memory, one contiguous cell per epoch
-        for (uint32_t i = lane; i < len; i += 32) {
-            const float per = sched[beg + i].y;
-            my[i] = make_float2(per, per);  // reset state: cursor = period
-        }
-        __syncwarp();
-        uint64_t bases = 0;  // lane l: the cell offset of epoch (e & ~31) + l
-        for (uint32_t e = 0; e < n_epochs; e++) {
-            const float ef = (float)e;
-            if (rec && (e & 31) == 0 && e + lane < n_epochs) bases = seg_ptr[(size_t)(e + lane) * nseg + s];
-            uint64_t pos = rec ? __shfl_sync(0xFFFFFFFFu, bases, e & 31) : 0;
-            uint32_t cnt = 0;
-            for (uint32_t i0 = 0; i0 < len; i0 += 32) {
-                const uint32_t i = i0 + lane;
-                bool a = false;
-                if (i < len) {
-                    float2 c = my[i];
-                    a = c.x <= ef;
-                    if (a) my[i].x = c.x + c.y;
-                }
-                const unsigned m = __ballot_sync(0xFFFFFFFFu, a);
-                if (rec && a) rec[pos + __popc(m & lt)] = make_uint2(beg + i, other[beg + i]);
-                pos += __popc(m);
-                cnt += __popc(m);
-            }
-            if (!rec && lane == 0) counts[(size_t)e * nseg + s] = cnt;
-        }
-        return;
+    for (uint32_t i = lane; i < len; i += 32) {
+        const float per = sched[beg + i].y;
+        my[i] = make_float2(per, per);  // reset state: cursor = period
     }
-    // chunk-major for long segments: per-epoch running counts in global
-    // memory order (chunk by chunk, CSR order within each cell)
-    uint32_t *run = reinterpret_cast<uint32_t *>(my);  // n_epochs <= 2 * kSchedCap words
-    for (uint32_t e = lane; e < n_epochs; e += 32) run[e] = 0;
     __syncwarp();
-    for (uint32_t c0 = beg; c0 < end; c0 += 32u) {
-        const uint32_t p = c0 + lane;
-        const bool live = p < end;
-        float c = 0.0f, per = 0.0f;
-        uint32_t o = 0;
-        if (live) {
-            per = sched[p].y;
-            c = per;
-            if (rec) o = other[p];
-        }
-        for (uint32_t e = 0; e < n_epochs; e++) {
-            const bool a = live && c <= (float)e;
-            if (a) c = c + per;
-            const unsigned m = __ballot_sync(0xFFFFFFFFu, a);
-            if (m) {
-                if (rec && a) rec[seg_ptr[(size_t)e * nseg + s] + run[e] + __popc(m & lt)] = make_uint2(p, o);
-                __syncwarp();
-                if (lane == 0) run[e] += __popc(m);
-                __syncwarp();
+    uint64_t bases = 0;  // lane l: the cell offset of epoch (e & ~31) + l
+    for (uint32_t e = 0; e < n_epochs; e++) {
+        const float ef = (float)e;
+        if (rec && (e & 31) == 0 && e + lane < n_epochs) bases = ptr[(size_t)(e + lane) * n_units + u];
+        uint64_t pos = rec ? __shfl_sync(0xFFFFFFFFu, bases, e & 31) : 0;
+        uint32_t cnt = 0;
+        for (uint32_t i0 = 0; i0 < len; i0 += 32) {
+            const uint32_t i = i0 + lane;
+            bool a = false;
+            if (i < len) {
+                const float2 c = my[i];
+                a = c.x <= ef;
+                if (a) my[i].x = c.x + c.y;
             }
+            const unsigned m = __ballot_sync(0xFFFFFFFFu, a);
+            if (rec && a) rec[pos + __popc(m & lt)] = make_uint2(beg + i, other[beg + i]);
+            pos += __popc(m);
+            cnt += __popc(m);
         }
-    }
-    if (!rec) {
-        __syncwarp();
-        for (uint32_t e = lane; e < n_epochs; e += 32) counts[(size_t)e * nseg + s] = run[e];
+        if (!rec && lane == 0) counts[(size_t)e * n_units + u] = cnt;
     }
 }
 
@@ -129,12 +116,7 @@ bool build_schedule_lists(const DeviceCsr &csr, uint32_t n_epochs, ScheduleLists
 {
     out = ScheduleLists();
     const uint32_t n = csr.n, nseg = ceil_div(n, 32);
-    if (!n || !n_epochs || n_epochs > 2 * kSchedCap || !csr.n_edges) return false;
-    const uint64_t cells = (uint64_t)n_epochs * nseg;
-    const size_t smem = (size_t)kSchedWarps * kSchedCap * sizeof(float2);
-    const unsigned grid = ceil_div(nseg, kSchedWarps);
-    check_cuda(cudaFuncSetAttribute(k_sched_lists, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-               "smem attribute");
+    if (!n || !n_epochs || n_epochs > 4096 || !csr.n_edges) return false;
     const bool timing = getenv("UMAPCU_TIMING") != nullptr;
     auto t0 = std::chrono::steady_clock::now();
     auto lap = [&](const char *what) {
@@ -145,14 +127,32 @@ bool build_schedule_lists(const DeviceCsr &csr, uint32_t n_epochs, ScheduleLists
                 std::chrono::duration<double, std::milli>(t1 - t0).count());
         t0 = t1;
     };
+    // work units per segment -> unit_base [nseg + 1]
+    DevBuf<uint32_t> units(nseg, s), unit_base(nseg + 1, s);
+    k_sched_units<<<ceil_div(nseg, 256), 256, 0, s>>>(csr.offsets.p, n, nseg, units.p);
+    check_launch("k_sched_units");
+    {
+        size_t tb = 0;
+        check_cuda(cub::DeviceScan::InclusiveSum(nullptr, tb, units.p, unit_base.p + 1, (int64_t)nseg, s), "scan size");
+        DevBuf<char> tmp(tb ? tb : 1, s);
+        check_cuda(cub::DeviceScan::InclusiveSum(tmp.p, tb, units.p, unit_base.p + 1, (int64_t)nseg, s), "scan");
+    }
+    check_cuda(cudaMemsetAsync(unit_base.p, 0, sizeof(uint32_t), s), "memset");
+    uint32_t n_units = 0;
+    d2h(&n_units, unit_base.p + nseg, 1, s);
+    sync(s);
+    const uint64_t cells = (uint64_t)n_epochs * n_units;
+    const size_t smem = (size_t)kSchedWarps * kSchedCap * sizeof(float2);
+    const unsigned grid = ceil_div(n_units, kSchedWarps);
+    check_cuda(cudaFuncSetAttribute(k_sched_lists, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+               "smem attribute");
     DevBuf<uint32_t> counts(cells, s);
-    lap("alloc");
-    k_sched_lists<<<grid, kSchedWarps * 32, smem, s>>>(csr.offsets.p, csr.other.p, csr.sched.p, n, nseg, n_epochs,
-                                                       counts.p, nullptr, nullptr);
+    lap("units");
+    k_sched_lists<<<grid, kSchedWarps * 32, smem, s>>>(csr.offsets.p, csr.other.p, csr.sched.p, n, nseg, unit_base.p,
+                                                       n_units, n_epochs, counts.p, nullptr, nullptr);
     check_launch("k_sched_lists count");
     lap("count");
     DevBuf<uint64_t> ptr(cells + 1, s);
-    check_cuda(cudaMemsetAsync(ptr.p + cells, 0, sizeof(uint64_t), s), "memset");
     {
         size_t tb = 0;
         check_cuda(cub::DeviceScan::ExclusiveSum(nullptr, tb, counts.p, ptr.p, (int64_t)cells, s), "scan size");
@@ -166,6 +166,7 @@ bool build_schedule_lists(const DeviceCsr &csr, uint32_t n_epochs, ScheduleLists
     sync(s);
     const uint64_t R = last_ptr + last_cnt;
     h2d(ptr.p + cells, &R, 1, s);
+    lap("scan");
     // the records must fit comfortably beside everything else
     size_t free_b = 0, total_b = 0;
     check_cuda(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
@@ -173,18 +174,19 @@ bool build_schedule_lists(const DeviceCsr &csr, uint32_t n_epochs, ScheduleLists
         sync(s);
         return false;
     }
-    lap("scan");
     DevBuf<uint2> rec(R ? R : 1, s);
     lap("alloc rec");
-    k_sched_lists<<<grid, kSchedWarps * 32, smem, s>>>(csr.offsets.p, csr.other.p, csr.sched.p, n, nseg, n_epochs,
-                                                       nullptr, ptr.p, rec.p);
+    k_sched_lists<<<grid, kSchedWarps * 32, smem, s>>>(csr.offsets.p, csr.other.p, csr.sched.p, n, nseg, unit_base.p,
+                                                       n_units, n_epochs, nullptr, ptr.p, rec.p);
     check_launch("k_sched_lists fill");
     lap("fill");
     out.rec = std::move(rec);
-    out.seg_ptr = std::move(ptr);
+    out.ptr = std::move(ptr);
+    out.unit_base = std::move(unit_base);
     out.n_records = R;
     out.n_epochs = n_epochs;
     out.nseg = nseg;
+    out.n_units = n_units;
     return true;
 }
 
