@@ -1,0 +1,346 @@
+// Spectral initialisation on the device: the smallest eigenpairs of a sparse
+// symmetric matrix by Lanczos with full reorthogonalisation
+// (compute_smallest_eigenpairs_lanczos, src/utils/math.rs:401-616), and the
+// layout built on them (spectral_layout, src/data/init.rs:986-1004: the
+// negative normalised adjacency -D^-1/2 A D^-1/2 per connected component,
+// eigenvectors 1..n_comp, centred, scaled to a range, small noise).
+//
+// Device side: CSR SpMV in f64, dot products, the two-pass classical
+// Gram-Schmidt against the whole Krylov basis (basis^T w, then w -= basis c,
+// twice: one pass over the basis each way instead of the reference's
+// sequential modified Gram-Schmidt; both keep the basis orthogonal to
+// rounding), the back-transformation basis * c. Host side: the small
+// tridiagonal eigenproblem (at most 4 k + 30 rows) by cyclic Jacobi
+// rotations, the selection, and the bookkeeping of connected components.
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+#include <vector>
+
+#include "internal.cuh"
+
+namespace umapcu {
+namespace {
+
+constexpr int kBlk = 256;
+
+// y = M x, one warp per row, f64
+__global__ void k_spmv(uint32_t n, const uint64_t *__restrict__ ptr, const uint32_t *__restrict__ col,
+                       const double *__restrict__ val, const double *__restrict__ x, double *__restrict__ y)
+{
+    const uint32_t row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (row >= n) return;
+    double acc = 0.0;
+    for (uint64_t p = ptr[row] + lane; p < ptr[row + 1]; p += 32) acc += val[p] * x[col[p]];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xFFFFFFFFu, acc, o);
+    if (lane == 0) y[row] = acc;
+}
+
+// out[j] = <V_j, w> for basis rows j < m: one block per row, fixed-order
+// block reduction
+__global__ void k_basis_dots(const double *__restrict__ V, uint32_t n, uint32_t m, const double *__restrict__ w,
+                             double *__restrict__ out)
+{
+    __shared__ double sh[kBlk];
+    const uint32_t j = blockIdx.x;
+    if (j >= m) return;
+    const double *v = V + (size_t)j * n;
+    double acc = 0.0;
+    for (uint32_t i = threadIdx.x; i < n; i += kBlk) acc += v[i] * w[i];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = kBlk / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[j] = sh[0];
+}
+
+// w -= sum_j c_j V_j (sub) or out = sum_j c_j V_j (!sub)
+__global__ void k_basis_comb(const double *__restrict__ V, uint32_t n, uint32_t m, const double *__restrict__ c,
+                             double *__restrict__ w, bool sub)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double acc = 0.0;
+    for (uint32_t j = 0; j < m; j++) acc += c[j] * V[(size_t)j * n + i];
+    w[i] = sub ? w[i] - acc : acc;
+}
+
+__global__ void k_scale(const double *__restrict__ x, uint32_t n, double s, double *__restrict__ dst)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = x[i] * s;
+}
+
+// Start vector: uniform in [-0.5, 0.5) from a counter-based SplitMix64
+// stream keyed by the seed (the reference draws it from StdRng; any start
+// vector with a component along the wanted eigenvectors converges to them).
+__global__ void k_random_start(double *__restrict__ v, uint32_t n, uint64_t seed)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint64_t z = seed + 0x9E3779B97F4A7C15ull * (uint64_t)(i + 1);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    v[i] = (double)(z >> 11) * (1.0 / 9007199254740992.0) - 0.5;
+}
+
+// Symmetric eigen-decomposition of a small dense matrix by cyclic Jacobi
+// rotations (Golub & Van Loan, Matrix Computations, section 8.5):
+// a [m * m] is destroyed; evals [m], evecs [m * m] column-major (column k is
+// the eigenvector of evals[k]).
+void jacobi_eigen(std::vector<double> &a, uint32_t m, std::vector<double> &evals, std::vector<double> &evecs)
+{
+    evecs.assign((size_t)m * m, 0.0);
+    for (uint32_t i = 0; i < m; i++) evecs[(size_t)i * m + i] = 1.0;
+    auto A = [&](uint32_t r, uint32_t c) -> double & { return a[(size_t)r * m + c]; };
+    for (int sweep = 0; sweep < 100; sweep++) {
+        double off = 0.0, tot = 0.0;
+        for (uint32_t r = 0; r < m; r++)
+            for (uint32_t c = 0; c < m; c++) {
+                tot += A(r, c) * A(r, c);
+                if (r != c) off += A(r, c) * A(r, c);
+            }
+        if (off <= 1e-30 * (tot > 0 ? tot : 1.0)) break;
+        for (uint32_t p = 0; p + 1 < m; p++)
+            for (uint32_t q = p + 1; q < m; q++) {
+                const double apq = A(p, q);
+                if (std::fabs(apq) < 1e-300) continue;
+                const double theta = (A(q, q) - A(p, p)) / (2.0 * apq);
+                const double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+                const double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
+                for (uint32_t k = 0; k < m; k++) {  // A := A J (columns p, q)
+                    const double akp = A(k, p), akq = A(k, q);
+                    A(k, p) = c * akp - s * akq;
+                    A(k, q) = s * akp + c * akq;
+                }
+                for (uint32_t k = 0; k < m; k++) {  // A := J^T A (rows p, q)
+                    const double apk = A(p, k), aqk = A(q, k);
+                    A(p, k) = c * apk - s * aqk;
+                    A(q, k) = s * apk + c * aqk;
+                }
+                for (uint32_t k = 0; k < m; k++) {  // V := V J
+                    double &vp = evecs[(size_t)p * m + k], &vq = evecs[(size_t)q * m + k];
+                    const double x = vp, y = vq;
+                    vp = c * x - s * y;
+                    vq = s * x + c * y;
+                }
+            }
+    }
+    evals.resize(m);
+    for (uint32_t i = 0; i < m; i++) evals[i] = A(i, i);
+}
+
+double dev_dot(const double *a, const double *b, uint32_t n, double *d_tmp, cudaStream_t s)
+{
+    k_basis_dots<<<1, kBlk, 0, s>>>(a, n, 1, b, d_tmp);
+    check_launch("k_basis_dots");
+    double h = 0.0;
+    d2h(&h, d_tmp, 1, s);
+    sync(s);
+    return h;
+}
+
+}  // namespace
+
+// Smallest n_components eigenpairs of a symmetric CSR matrix (f64 values) on
+// the device: compute_smallest_eigenpairs_lanczos (src/utils/math.rs:401-616)
+// -- min(4 n_components + 30, n) Lanczos steps, early stop when beta < 1e-12,
+// the tridiagonal problem on the host, Ritz values ascending, Ritz vectors
+// back-transformed through the basis and normalised. evals [k], evecs
+// [n * k] (row i = point i, the reference's transposed output); k <=
+// n_components (fewer after an early breakdown, as in the reference).
+void smallest_eigenpairs_dev(uint32_t n, const uint64_t *d_ptr, const uint32_t *d_col, const double *d_val,
+                             uint32_t n_components, uint64_t seed, std::vector<float> &evals,
+                             std::vector<float> &evecs, uint32_t &k_out, cudaStream_t s)
+{
+    if (n == 0) fail(UMAPCU_NO_DATA, "eigenpairs of an empty matrix");
+    const uint32_t n_iter = std::min<uint32_t>(n_components * 4 + 30, n);
+    DevBuf<double> V((size_t)n_iter * n, s), w(n, s), c(n_iter, s), tmp(1, s);
+    const unsigned g = ceil_div(n, kBlk);
+    k_random_start<<<g, kBlk, 0, s>>>(V.p, n, seed);
+    check_launch("k_random_start");
+    {
+        const double nr = std::sqrt(dev_dot(V.p, V.p, n, tmp.p, s));
+        k_scale<<<g, kBlk, 0, s>>>(V.p, n, nr > 0 ? 1.0 / nr : 1.0, V.p);
+    }
+    std::vector<double> alpha, beta, hc(n_iter);
+    uint32_t n_done = 0;
+    for (uint32_t j = 0; j < n_iter; j++) {
+        double *vj = V.p + (size_t)j * n;
+        n_done = j + 1;
+        k_spmv<<<ceil_div((uint64_t)n * 32, kBlk), kBlk, 0, s>>>(n, d_ptr, d_col, d_val, vj, w.p);
+        check_launch("k_spmv");
+        const double a = dev_dot(w.p, vj, n, tmp.p, s);
+        alpha.push_back(a);
+        // w -= alpha v_j + beta_{j-1} v_{j-1}
+        std::fill(hc.begin(), hc.end(), 0.0);
+        hc[j] = a;
+        if (j) hc[j - 1] = beta[j - 1];
+        h2d(c.p, hc.data(), j + 1, s);
+        k_basis_comb<<<g, kBlk, 0, s>>>(V.p, n, j + 1, c.p, w.p, true);
+        // full reorthogonalisation: two classical Gram-Schmidt passes
+        for (int pass = 0; pass < 2; pass++) {
+            k_basis_dots<<<j + 1, kBlk, 0, s>>>(V.p, n, j + 1, w.p, c.p);
+            k_basis_comb<<<g, kBlk, 0, s>>>(V.p, n, j + 1, c.p, w.p, true);
+        }
+        check_launch("reorthogonalise");
+        const double b = std::sqrt(dev_dot(w.p, w.p, n, tmp.p, s));
+        beta.push_back(b);
+        if (b < 1e-12) break;
+        if (j + 1 < n_iter) {
+            k_scale<<<g, kBlk, 0, s>>>(w.p, n, 1.0 / b, V.p + (size_t)(j + 1) * n);
+            check_launch("k_scale");
+        }
+    }
+    const uint32_t m = n_done;
+    std::vector<double> T((size_t)m * m, 0.0), tev, tvec;
+    for (uint32_t i = 0; i < m; i++) {
+        T[(size_t)i * m + i] = alpha[i];
+        if (i + 1 < m) T[(size_t)i * m + i + 1] = T[(size_t)(i + 1) * m + i] = beta[i];
+    }
+    jacobi_eigen(T, m, tev, tvec);
+    std::vector<uint32_t> order(m);
+    std::iota(order.begin(), order.end(), 0u);
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return tev[x] < tev[y]; });
+    const uint32_t k = std::min(n_components, m);
+    evals.resize(k);
+    evecs.assign((size_t)n * k, 0.0f);
+    std::vector<double> hv(n);
+    for (uint32_t q = 0; q < k; q++) {
+        const uint32_t idx = order[q];
+        h2d(c.p, tvec.data() + (size_t)idx * m, m, s);
+        k_basis_comb<<<g, kBlk, 0, s>>>(V.p, n, m, c.p, w.p, false);
+        check_launch("k_basis_comb");
+        d2h(hv.data(), w.p, n, s);
+        sync(s);
+        double nrm = 0.0;
+        for (double x : hv) nrm += x * x;
+        nrm = std::sqrt(nrm);
+        for (uint32_t i = 0; i < n; i++) evecs[(size_t)i * k + q] = (float)(nrm > 0 ? hv[i] / nrm : hv[i]);
+        evals[q] = (float)tev[idx];
+    }
+    k_out = k;
+}
+
+namespace {
+
+// -D^-1/2 A D^-1/2 of a COO graph on n nodes (graph_to_negative_normalised_
+// adjacency, src/data/init.rs:210-256): degrees include self loops, the
+// matrix drops them; CSR rows keep the input order. Host arrays in, device
+// CSR out.
+void neg_normalised_adjacency(uint32_t n, uint64_t nnz, const uint32_t *row, const uint32_t *col, const float *w,
+                              DevBuf<uint64_t> &ptr, DevBuf<uint32_t> &cidx, DevBuf<double> &val, cudaStream_t s)
+{
+    std::vector<double> deg(n, 0.0);
+    for (uint64_t e = 0; e < nnz; e++) deg[row[e]] += (double)w[e];
+    std::vector<double> dis(n);
+    for (uint32_t i = 0; i < n; i++) dis[i] = deg[i] > 1e-8 ? 1.0 / std::sqrt(deg[i]) : 0.0;
+    std::vector<uint64_t> hp(n + 1, 0);
+    for (uint64_t e = 0; e < nnz; e++)
+        if (row[e] != col[e]) hp[row[e] + 1]++;
+    for (uint32_t i = 0; i < n; i++) hp[i + 1] += hp[i];
+    const uint64_t m = hp[n];
+    std::vector<uint32_t> hc(m ? m : 1);
+    std::vector<double> hv(m ? m : 1);
+    std::vector<uint64_t> fill(hp.begin(), hp.end() - 1);
+    for (uint64_t e = 0; e < nnz; e++) {
+        const uint32_t i = row[e], j = col[e];
+        if (i == j) continue;
+        const uint64_t q = fill[i]++;
+        hc[q] = j;
+        hv[q] = -dis[i] * (double)w[e] * dis[j];
+    }
+    ptr.alloc(n + 1, s);
+    cidx.alloc(hc.size(), s);
+    val.alloc(hv.size(), s);
+    h2d(ptr.p, hp.data(), n + 1, s);
+    h2d(cidx.p, hc.data(), hc.size(), s);
+    h2d(val.p, hv.data(), hv.size(), s);
+    sync(s);  // the host vectors go out of scope
+}
+
+// Deterministic host stream for the random fallbacks and the noise
+// (SplitMix64; the reference's StdRng streams are not reproduced).
+struct Mix {
+    uint64_t x;
+    uint64_t next()
+    {
+        uint64_t z = (x += 0x9E3779B97F4A7C15ull);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        return z ^ (z >> 31);
+    }
+    double uniform() { return (double)(next() >> 11) * (1.0 / 9007199254740992.0); }
+    double normal()  // Box-Muller
+    {
+        double u1 = uniform(), u2 = uniform();
+        if (u1 < 1e-300) u1 = 1e-300;
+        return std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2);
+    }
+};
+
+// single_component_spectral_raw (src/data/init.rs:276-320): eigenvectors
+// 1..n_comp of the component's -D^-1/2 A D^-1/2; graphs of at most n_comp + 1
+// points and dimensions Lanczos did not supply are uniform in [-1, 1).
+void component_raw(uint32_t n, uint64_t nnz, const uint32_t *row, const uint32_t *col, const float *w,
+                   uint32_t n_comp, uint64_t seed, std::vector<double> &out, cudaStream_t s)
+{
+    out.assign((size_t)n * n_comp, 0.0);
+    if (n <= n_comp + 1) {
+        Mix r{seed};
+        for (double &v : out) v = 2.0 * r.uniform() - 1.0;
+        return;
+    }
+    DevBuf<uint64_t> ptr;
+    DevBuf<uint32_t> ci;
+    DevBuf<double> val;
+    neg_normalised_adjacency(n, nnz, row, col, w, ptr, ci, val, s);
+    std::vector<float> ev, vec;
+    uint32_t k = 0;
+    smallest_eigenpairs_dev(n, ptr.p, ci.p, val.p, std::min(n_comp + 1, n), seed, ev, vec, k, s);
+    for (uint32_t d = 0; d < n_comp; d++) {
+        if (d + 1 < k) {
+            for (uint32_t i = 0; i < n; i++) out[(size_t)i * n_comp + d] = vec[(size_t)i * k + d + 1];
+        } else {
+            Mix r{seed + d};
+            for (uint32_t i = 0; i < n; i++) out[(size_t)i * n_comp + d] = 2.0 * r.uniform() - 1.0;
+        }
+    }
+}
+
+double max_abs(const std::vector<double> &v)
+{
+    double m = 0.0;
+    for (double x : v) m = std::max(m, std::fabs(x));
+    return m;
+}
+
+// centre every dimension, then scale so the largest |coordinate| is range
+void centre_and_scale(std::vector<double> &e, uint32_t n, uint32_t n_comp, double range)
+{
+    for (uint32_t d = 0; d < n_comp; d++) {
+        double mean = 0.0;
+        for (uint32_t i = 0; i < n; i++) mean += e[(size_t)i * n_comp + d];
+        mean /= n;
+        for (uint32_t i = 0; i < n; i++) e[(size_t)i * n_comp + d] -= mean;
+    }
+    const double m = max_abs(e);
+    if (m > 1e-8)
+        for (double &x : e) x *= range / m;
+}
+
+uint32_t uf_find(std::vector<uint32_t> &p, uint32_t x)
+{
+    while (p[x] != x) {
+        p[x] = p[p[x]];
+        x = p[x];
+    }
+    return x;
+}
+
+}  // namespace
+}  // namespace umapcu
