@@ -418,6 +418,30 @@ umapcu_status umapcu_knn_save(const char *path, uint32_t n, uint32_t k, uint32_t
 umapcu_status umapcu_knn_load_header(const char *path, uint32_t *n, uint32_t *k, uint32_t *metric);
 umapcu_status umapcu_knn_load(const char *path, uint32_t n, uint32_t k, int32_t *knn_idx, float *knn_dist);
 
+/* ------------------------------------------------------- spectral init */
+
+/* Smallest eigenpairs of a symmetric sparse matrix (CSR host arrays, f64
+ * values): replaces compute_smallest_eigenpairs_lanczos
+ * (src/utils/math.rs:617-628). min(4 k + 30, n) Lanczos steps on the device
+ * with full reorthogonalisation, early stop on breakdown. evals [k]
+ * ascending, evecs [n * k] (row i = point i); *n_found <= n_components
+ * (fewer after an early breakdown, as in the reference). */
+umapcu_status umapcu_smallest_eigenpairs(uint32_t n, const uint64_t *ptr, const uint32_t *col, const double *val,
+                                         uint32_t n_components, uint64_t seed, float *evals, float *evecs,
+                                         uint32_t *n_found);
+
+/* Spectral initialisation of a symmetric graph (COO host arrays): replaces
+ * spectral_layout without a data matrix (src/data/init.rs:986-1004).
+ * Connected: eigenvectors 1..n_comp of -D^-1/2 A D^-1/2, centred, scaled so
+ * the largest |coordinate| is `range` (<= 0: 10), plus N(0, 1e-4) noise.
+ * Several components: centroids on the simplex, each component's spectral
+ * layout (random when it has fewer than 2 n_comp points) around its
+ * centroid, then centred and scaled. embd [n * n_comp]. The Lanczos start
+ * vector, the random fallbacks and the noise come from this library's own
+ * seeded streams, not the reference's StdRng. */
+umapcu_status umapcu_spectral_layout(const uint32_t *row, const uint32_t *col, const float *val, uint64_t nnz,
+                                     uint32_t n, uint32_t n_comp, uint64_t seed, float range, float *embd);
+
 #ifdef __cplusplus
 }
 #endif

@@ -344,3 +344,163 @@ uint32_t uf_find(std::vector<uint32_t> &p, uint32_t x)
 
 }  // namespace
 }  // namespace umapcu
+
+using namespace umapcu;
+
+namespace {
+
+template <typename F>
+umapcu_status guard_s(F &&f)
+{
+    try {
+        return f();
+    } catch (const Error &e) {
+        return e.status;
+    } catch (const std::bad_alloc &) {
+        return UMAPCU_CUDA_ALLOC;
+    } catch (...) {
+        return UMAPCU_CUDA_LAUNCH;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+umapcu_status umapcu_smallest_eigenpairs(uint32_t n, const uint64_t *ptr, const uint32_t *col, const double *val,
+                                         uint32_t n_components, uint64_t seed, float *evals, float *evecs,
+                                         uint32_t *n_found)
+{
+    return guard_s([&]() -> umapcu_status {
+        if (n == 0) return UMAPCU_NO_DATA;
+        if (!ptr || !evals || !evecs || !n_found || n_components == 0 || n_components > 128) return UMAPCU_BAD_ARG;
+        const uint64_t nnz = ptr[n];
+        if (nnz && (!col || !val)) return UMAPCU_BAD_ARG;
+        for (uint32_t i = 0; i < n; i++)
+            if (ptr[i + 1] < ptr[i]) return UMAPCU_BAD_ARG;
+        for (uint64_t e = 0; e < nnz; e++)
+            if (col[e] >= n) return UMAPCU_BAD_ARG;
+        Stream st;
+        DevBuf<uint64_t> dp(n + 1, st.s);
+        DevBuf<uint32_t> dc(nnz ? nnz : 1, st.s);
+        DevBuf<double> dv(nnz ? nnz : 1, st.s);
+        h2d(dp.p, ptr, n + 1, st.s);
+        h2d(dc.p, col, nnz, st.s);
+        h2d(dv.p, val, nnz, st.s);
+        std::vector<float> ev, vec;
+        uint32_t k = 0;
+        smallest_eigenpairs_dev(n, dp.p, dc.p, dv.p, n_components, seed, ev, vec, k, st.s);
+        std::copy(ev.begin(), ev.end(), evals);
+        std::copy(vec.begin(), vec.end(), evecs);  // [n][k]
+        *n_found = k;
+        return UMAPCU_OK;
+    });
+}
+
+umapcu_status umapcu_spectral_layout(const uint32_t *row, const uint32_t *col, const float *val, uint64_t nnz,
+                                     uint32_t n, uint32_t n_comp, uint64_t seed, float range, float *embd)
+{
+    return guard_s([&]() -> umapcu_status {
+        if (n == 0) return UMAPCU_NO_DATA;
+        if (!embd || n_comp == 0 || n_comp > 64 || (nnz && (!row || !col || !val))) return UMAPCU_BAD_ARG;
+        for (uint64_t e = 0; e < nnz; e++)
+            if (row[e] >= n || col[e] >= n) return UMAPCU_BAD_ARG;
+        const double rng = range > 0.0f ? (double)range : 10.0;  // SPECTRAL_RANGE, init.rs:17
+        Stream st;
+        // connected components (find_connected_components, init.rs:349-391),
+        // labelled in order of their smallest point, members ascending
+        std::vector<uint32_t> par(n);
+        std::iota(par.begin(), par.end(), 0u);
+        for (uint64_t e = 0; e < nnz; e++) {
+            const uint32_t a = uf_find(par, row[e]), b = uf_find(par, col[e]);
+            if (a != b) par[std::max(a, b)] = std::min(a, b);
+        }
+        std::vector<uint32_t> label(n), local(n), cid(n, ~0u);
+        std::vector<std::vector<uint32_t>> members;
+        for (uint32_t i = 0; i < n; i++) {
+            const uint32_t r = uf_find(par, i);
+            if (cid[r] == ~0u) {
+                cid[r] = (uint32_t)members.size();
+                members.emplace_back();
+            }
+            label[i] = cid[r];
+            local[i] = (uint32_t)members[label[i]].size();
+            members[label[i]].push_back(i);
+        }
+        std::vector<double> out((size_t)n * n_comp, 0.0);
+        if (members.size() == 1) {
+            // single_component_spectral + finalise_spectral_embedding
+            // (init.rs:876-958): centre, scale to range, N(0, 1e-4) noise
+            component_raw(n, nnz, row, col, val, n_comp, seed, out, st.s);
+            centre_and_scale(out, n, n_comp, rng);
+            Mix r{seed + 9999};
+            for (double &x : out) x += 1e-4 * r.normal();
+        } else {
+            // multi_component_init (init.rs:413-524) without a data matrix:
+            // centroids on the simplex (component_simplex_meta, init.rs:614),
+            // each component spectral around its centroid within half the
+            // largest centroid distance (random when it has fewer than
+            // 2 n_comp points), then the whole centred and scaled
+            const uint32_t C = (uint32_t)members.size(), half = (C + 1) / 2;
+            std::vector<double> meta((size_t)C * n_comp, 0.0);
+            for (uint32_t c = 0; c < C; c++) {
+                const uint32_t idx = c < half ? c : c - half;
+                if (idx < n_comp) meta[(size_t)c * n_comp + idx] = c < half ? 1.0 : -1.0;
+            }
+            const double mm = max_abs(meta);
+            if (mm > 1e-8)
+                for (double &x : meta) x /= mm;
+            std::vector<uint64_t> cnt(C + 1, 0);
+            for (uint64_t e = 0; e < nnz; e++)
+                if (label[row[e]] == label[col[e]]) cnt[label[row[e]] + 1]++;
+            for (uint32_t c = 0; c < C; c++) cnt[c + 1] += cnt[c];
+            const size_t m = cnt[C] ? cnt[C] : 1;
+            std::vector<uint32_t> sr(m), sc(m);
+            std::vector<float> sw(m);
+            std::vector<uint64_t> at(cnt.begin(), cnt.end() - 1);
+            for (uint64_t e = 0; e < nnz; e++) {
+                const uint32_t c = label[row[e]];
+                if (c != label[col[e]]) continue;
+                const uint64_t q = at[c]++;
+                sr[q] = local[row[e]];
+                sc[q] = local[col[e]];
+                sw[q] = val[e];
+            }
+            Mix r{seed};
+            for (uint32_t c = 0; c < C; c++) {
+                const double *cen = meta.data() + (size_t)c * n_comp;
+                double dr = 0.0;  // meta_data_range (init.rs:768)
+                for (uint32_t o = 0; o < C; o++) {
+                    double d2 = 0.0;
+                    for (uint32_t d = 0; d < n_comp; d++) {
+                        const double df = cen[d] - meta[(size_t)o * n_comp + d];
+                        d2 += df * df;
+                    }
+                    dr = std::max(dr, std::sqrt(d2));
+                }
+                dr /= 2.0;
+                const std::vector<uint32_t> &mem = members[c];
+                const uint32_t nc = (uint32_t)mem.size();
+                if (nc < 2 * n_comp) {
+                    for (uint32_t gi : mem)
+                        for (uint32_t d = 0; d < n_comp; d++)
+                            out[(size_t)gi * n_comp + d] = cen[d] + (2.0 * r.uniform() - 1.0) * dr;
+                    continue;
+                }
+                std::vector<double> sub;
+                component_raw(nc, cnt[c + 1] - cnt[c], sr.data() + cnt[c], sc.data() + cnt[c], sw.data() + cnt[c],
+                              n_comp, seed + c, sub, st.s);
+                const double sm = max_abs(sub);
+                const double ex = sm > 1e-8 ? dr / sm : 1.0;
+                for (uint32_t li = 0; li < nc; li++)
+                    for (uint32_t d = 0; d < n_comp; d++)
+                        out[(size_t)mem[li] * n_comp + d] = cen[d] + sub[(size_t)li * n_comp + d] * ex;
+            }
+            centre_and_scale(out, n, n_comp, rng);
+        }
+        for (size_t i = 0; i < out.size(); i++) embd[i] = (float)out[i];
+        return UMAPCU_OK;
+    });
+}
+
+}  // extern "C"

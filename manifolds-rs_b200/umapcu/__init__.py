@@ -144,6 +144,8 @@ _SIGS = {
     "umapcu_eval_pow": [_vp, _u32, _f32, _i32, _vp],
     "umapcu_knn_exact": [_vp, _u32, _u32, _u32, _u32, _vp, _vp],
     "umapcu_state_schedule_info": [_vp, _vp, _vp, _vp],
+    "umapcu_smallest_eigenpairs": [_u32, _vp, _vp, _vp, _u32, _u64, _vp, _vp, _vp],
+    "umapcu_spectral_layout": [_vp, _vp, _vp, _u64, _u32, _u32, _u64, _f32, _vp],
     "umapcu_knn_exact_dev": [_vp, _u32, _u32, _vp, _u32, _u32, _u32, _vp, _vp, _vp],
     "umapcu_embedding_quality": [_vp, _u32, _u32, _vp, _u32, _vp, _u32, _u32, _vp, _u32, _u32, _vp, _vp],
     "umapcu_fuzzy_cross_entropy": [_vp, _vp, _vp, _u64, _vp, _u32, _u32, _f32, _f32, _vp],
@@ -781,3 +783,34 @@ def load_knn(path: str):
     d = np.empty((n.value, k.value), np.float32)
     _check(_lib.umapcu_knn_load(bp, n.value, k.value, _p(i), _p(d)), "knn_load")
     return i, d, m.value
+
+
+# ------------------------------------------------------------ spectral init
+
+def compute_smallest_eigenpairs_lanczos(ptr, col, val, n_components: int, seed: int = 42):
+    """compute_smallest_eigenpairs_lanczos (src/utils/math.rs:617) on the GPU
+    for a CSR matrix: -> (evals [k] ascending, evecs [n, k])."""
+    p = _c(ptr, np.uint64)
+    n = p.size - 1
+    c = _c(col, np.uint32)
+    v = _c(val, np.float64)
+    ev = np.empty(n_components, np.float32)
+    vec = np.empty(n * n_components, np.float32)
+    k = C.c_uint32()
+    _check(_lib.umapcu_smallest_eigenpairs(n, _p(p), _p(c), _p(v), n_components, int(seed) & (2 ** 64 - 1),
+                                           _p(ev), _p(vec), C.byref(k)), "smallest_eigenpairs")
+    kk = k.value
+    return ev[:kk].copy(), vec[: n * kk].reshape(n, kk).copy()
+
+
+def spectral_layout(graph: "CoordinateList", n_comp: int = 2, seed: int = 42, range_: float = 10.0):
+    """spectral_layout (src/data/init.rs:986) without a data matrix, on the
+    GPU: -> embedding [n, n_comp] f32."""
+    r = _c(graph.row_indices, np.uint32)
+    c = _c(graph.col_indices, np.uint32)
+    w = _c(graph.values, np.float32)
+    n = int(graph.n_samples)
+    out = np.empty((n, n_comp), np.float32)
+    _check(_lib.umapcu_spectral_layout(_p(r), _p(c), _p(w), r.size, n, n_comp, int(seed) & (2 ** 64 - 1),
+                                       float(range_), _p(out)), "spectral_layout")
+    return out
