@@ -445,3 +445,49 @@ def knn_preservation(knn_idx, Y, k=15, queries=None):
     rows = np.arange(Y.shape[0]) if queries is None else np.asarray(queries)
     kx = np.asarray(knn_idx)[rows, :k]
     return float(np.mean([len(set(a.tolist()) & set(b.tolist())) / k for a, b in zip(kx, ynbr)]))
+
+
+# ------------------------------------------------------- spectral init
+
+def splitmix_start(n, seed):
+    """The library's Lanczos start vector: uniform in [-0.5, 0.5) from the
+    counter-based SplitMix64 stream (the reference draws it from StdRng)."""
+    i = np.arange(1, n + 1, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        z = np.uint64(seed) + np.uint64(0x9E3779B97F4A7C15) * i
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z ^= z >> np.uint64(31)
+    return (z >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0) - 0.5
+
+
+def lanczos_smallest(M, k, start):
+    """lanczos_eigendecomp + select_eigenpairs (src/utils/math.rs:401-616),
+    restated with numpy: min(4 k + 30, n) steps from `start`, modified
+    Gram-Schmidt against the whole basis, stop when beta < 1e-12; Ritz
+    values ascending and unit Ritz vectors [n, k]. M: dense or scipy."""
+    n = M.shape[0]
+    n_iter = min(4 * k + 30, n)
+    v = start / np.linalg.norm(start)
+    basis, alpha, beta = [], [], []
+    v_old = np.zeros(n)
+    for j in range(n_iter):
+        basis.append(v.copy())
+        w = M @ v
+        a = float(w @ v)
+        alpha.append(a)
+        w = w - a * v - (beta[j - 1] * v_old if j else 0.0)
+        for b in basis:
+            w = w - float(w @ b) * b
+        bt = float(np.linalg.norm(w))
+        beta.append(bt)
+        if bt < 1e-12:
+            break
+        v_old, v = v, w / bt
+    m = len(alpha)
+    T = np.diag(alpha) + np.diag(beta[:m - 1], 1) + np.diag(beta[:m - 1], -1)
+    tw, tv = np.linalg.eigh(T)
+    sel = np.argsort(tw, kind="stable")[:min(k, m)]
+    V = np.array(basis).T @ tv[:, sel]
+    V /= np.linalg.norm(V, axis=0, keepdims=True)
+    return tw[sel], V
