@@ -11,11 +11,13 @@
 // sequential modified Gram-Schmidt; both keep the basis orthogonal to
 // rounding), the back-transformation basis * c. Host side: the small
 // tridiagonal eigenproblem (at most 4 k + 30 rows) by cyclic Jacobi
-// rotations, the selection, and the bookkeeping of connected components.
+// rotations, the selection, and the placement of several components.
 #include <algorithm>
 #include <cmath>
 #include <numeric>
 #include <vector>
+
+#include <cub/cub.cuh>
 
 #include "internal.cuh"
 
@@ -228,39 +230,147 @@ void smallest_eigenpairs_dev(uint32_t n, const uint64_t *d_ptr, const uint32_t *
 
 namespace {
 
+__global__ void k_iota(uint32_t *__restrict__ v, uint64_t m)
+{
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m) v[i] = (uint32_t)i;
+}
+
+__global__ void k_row_count(const uint32_t *__restrict__ row, uint64_t m, unsigned long long *__restrict__ cnt)
+{
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m) atomicAdd(&cnt[row[i]], 1ull);
+}
+
+// CSR (input order within rows) gathered through the stable row sort
+__global__ void k_csr_gather(const uint32_t *__restrict__ perm, uint64_t m, const uint32_t *__restrict__ col,
+                             const float *__restrict__ w, uint32_t *__restrict__ ccol, double *__restrict__ cw)
+{
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    const uint32_t e = perm[i];
+    ccol[i] = col[e];
+    cw[i] = (double)w[e];
+}
+
+// D^-1/2 from the row sums (self loops included), per row in CSR order
+__global__ void k_deg_inv_sqrt(uint32_t n, const uint64_t *__restrict__ ptr, const double *__restrict__ cw,
+                               double *__restrict__ dis)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double d = 0.0;
+    for (uint64_t p = ptr[i]; p < ptr[i + 1]; p++) d += cw[p];
+    dis[i] = d > 1e-8 ? 1.0 / sqrt(d) : 0.0;
+}
+
+// values -D^-1/2 w D^-1/2, self loops zero (the matrix has none)
+__global__ void k_neg_norm_values(uint32_t n, const uint64_t *__restrict__ ptr, const uint32_t *__restrict__ ccol,
+                                  const double *__restrict__ dis, double *__restrict__ cw)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (uint64_t p = ptr[i]; p < ptr[i + 1]; p++) {
+        const uint32_t j = ccol[p];
+        cw[p] = i == j ? 0.0 : -dis[i] * cw[p] * dis[j];
+    }
+}
+
 // -D^-1/2 A D^-1/2 of a COO graph on n nodes (graph_to_negative_normalised_
-// adjacency, src/data/init.rs:210-256): degrees include self loops, the
-// matrix drops them; CSR rows keep the input order. Host arrays in, device
-// CSR out.
+// adjacency, src/data/init.rs:210-256) built on the device: degrees include
+// self loops, self-loop entries carry 0 (the reference drops them), CSR rows
+// keep the input order (stable sort by row). Host arrays in, device CSR out.
 void neg_normalised_adjacency(uint32_t n, uint64_t nnz, const uint32_t *row, const uint32_t *col, const float *w,
                               DevBuf<uint64_t> &ptr, DevBuf<uint32_t> &cidx, DevBuf<double> &val, cudaStream_t s)
 {
-    std::vector<double> deg(n, 0.0);
-    for (uint64_t e = 0; e < nnz; e++) deg[row[e]] += (double)w[e];
-    std::vector<double> dis(n);
-    for (uint32_t i = 0; i < n; i++) dis[i] = deg[i] > 1e-8 ? 1.0 / std::sqrt(deg[i]) : 0.0;
-    std::vector<uint64_t> hp(n + 1, 0);
-    for (uint64_t e = 0; e < nnz; e++)
-        if (row[e] != col[e]) hp[row[e] + 1]++;
-    for (uint32_t i = 0; i < n; i++) hp[i + 1] += hp[i];
-    const uint64_t m = hp[n];
-    std::vector<uint32_t> hc(m ? m : 1);
-    std::vector<double> hv(m ? m : 1);
-    std::vector<uint64_t> fill(hp.begin(), hp.end() - 1);
-    for (uint64_t e = 0; e < nnz; e++) {
-        const uint32_t i = row[e], j = col[e];
-        if (i == j) continue;
-        const uint64_t q = fill[i]++;
-        hc[q] = j;
-        hv[q] = -dis[i] * (double)w[e] * dis[j];
-    }
+    const uint64_t m = nnz ? nnz : 1;
+    DevBuf<uint32_t> drow(m, s), dcol(m, s), rs(m, s), perm0(m, s), perm(m, s);
+    DevBuf<float> dw(m, s);
+    h2d(drow.p, row, nnz, s);
+    h2d(dcol.p, col, nnz, s);
+    h2d(dw.p, w, nnz, s);
+    DevBuf<unsigned long long> cnt(n + 1, s);
+    check_cuda(cudaMemsetAsync(cnt.p, 0, sizeof(unsigned long long) * (n + 1), s), "memset");
     ptr.alloc(n + 1, s);
-    cidx.alloc(hc.size(), s);
-    val.alloc(hv.size(), s);
-    h2d(ptr.p, hp.data(), n + 1, s);
-    h2d(cidx.p, hc.data(), hc.size(), s);
-    h2d(val.p, hv.data(), hv.size(), s);
-    sync(s);  // the host vectors go out of scope
+    cidx.alloc(m, s);
+    val.alloc(m, s);
+    if (nnz) {
+        const unsigned g = ceil_div(nnz, kBlk);
+        k_iota<<<g, kBlk, 0, s>>>(perm0.p, nnz);
+        size_t tb = 0;
+        int bits = 1;
+        while (bits < 32 && (1ull << bits) <= n) bits++;
+        check_cuda(cub::DeviceRadixSort::SortPairs(nullptr, tb, drow.p, rs.p, perm0.p, perm.p, (int64_t)nnz, 0, bits,
+                                                   s), "sort size");
+        {
+            DevBuf<char> tmp(tb ? tb : 1, s);
+            check_cuda(cub::DeviceRadixSort::SortPairs(tmp.p, tb, drow.p, rs.p, perm0.p, perm.p, (int64_t)nnz, 0, bits,
+                                                       s), "sort");
+        }
+        k_row_count<<<g, kBlk, 0, s>>>(drow.p, nnz, cnt.p + 1);
+        k_csr_gather<<<g, kBlk, 0, s>>>(perm.p, nnz, dcol.p, dw.p, cidx.p, val.p);
+        check_launch("csr gather");
+    }
+    {
+        size_t tb = 0;
+        check_cuda(cub::DeviceScan::InclusiveSum(nullptr, tb, cnt.p, (unsigned long long *)ptr.p, (int64_t)(n + 1), s),
+                   "scan size");
+        DevBuf<char> tmp(tb ? tb : 1, s);
+        check_cuda(cub::DeviceScan::InclusiveSum(tmp.p, tb, cnt.p, (unsigned long long *)ptr.p, (int64_t)(n + 1), s),
+                   "scan");
+    }
+    DevBuf<double> dis(n, s);
+    k_deg_inv_sqrt<<<ceil_div(n, kBlk), kBlk, 0, s>>>(n, ptr.p, val.p, dis.p);
+    k_neg_norm_values<<<ceil_div(n, kBlk), kBlk, 0, s>>>(n, ptr.p, cidx.p, dis.p, val.p);
+    check_launch("neg normalised adjacency");
+}
+
+// Connected-component labels on the device: every point starts with its own
+// index, edges pull both endpoints to the smaller label and labels follow
+// their labels' labels until nothing changes; each point ends with the
+// smallest index of its component. Host labels out.
+__global__ void k_cc_hook(const uint32_t *__restrict__ row, const uint32_t *__restrict__ col, uint64_t m,
+                          uint32_t *__restrict__ lab, uint32_t *__restrict__ changed)
+{
+    const uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= m) return;
+    const uint32_t a = lab[row[e]], b = lab[col[e]];
+    if (a == b) return;
+    const uint32_t lo = min(a, b), hi = max(a, b);
+    atomicMin(&lab[hi], lo);
+    *changed = 1u;
+}
+
+__global__ void k_cc_jump(uint32_t *__restrict__ lab, uint32_t n)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t l = lab[i];
+    while (lab[l] != l) l = lab[l];
+    lab[i] = l;
+}
+
+void component_labels(uint32_t n, uint64_t nnz, const uint32_t *row, const uint32_t *col,
+                      std::vector<uint32_t> &labels, cudaStream_t s)
+{
+    const uint64_t m = nnz ? nnz : 1;
+    DevBuf<uint32_t> drow(m, s), dcol(m, s), lab(n, s), changed(1, s);
+    h2d(drow.p, row, nnz, s);
+    h2d(dcol.p, col, nnz, s);
+    k_iota<<<ceil_div(n, kBlk), kBlk, 0, s>>>(lab.p, n);
+    for (uint32_t it = 0; nnz && it < 4096; it++) {
+        uint32_t h = 0;
+        check_cuda(cudaMemsetAsync(changed.p, 0, sizeof(uint32_t), s), "memset");
+        k_cc_hook<<<ceil_div(nnz, kBlk), kBlk, 0, s>>>(drow.p, dcol.p, nnz, lab.p, changed.p);
+        k_cc_jump<<<ceil_div(n, kBlk), kBlk, 0, s>>>(lab.p, n);
+        check_launch("components");
+        d2h(&h, changed.p, 1, s);
+        sync(s);
+        if (!h) break;
+    }
+    labels.resize(n);
+    d2h(labels.data(), lab.p, n, s);
+    sync(s);
 }
 
 // Deterministic host stream for the random fallbacks and the noise
@@ -333,14 +443,6 @@ void centre_and_scale(std::vector<double> &e, uint32_t n, uint32_t n_comp, doubl
         for (double &x : e) x *= range / m;
 }
 
-uint32_t uf_find(std::vector<uint32_t> &p, uint32_t x)
-{
-    while (p[x] != x) {
-        p[x] = p[p[x]];
-        x = p[x];
-    }
-    return x;
-}
 
 }  // namespace
 }  // namespace umapcu
@@ -409,16 +511,12 @@ umapcu_status umapcu_spectral_layout(const uint32_t *row, const uint32_t *col, c
         Stream st;
         // connected components (find_connected_components, init.rs:349-391),
         // labelled in order of their smallest point, members ascending
-        std::vector<uint32_t> par(n);
-        std::iota(par.begin(), par.end(), 0u);
-        for (uint64_t e = 0; e < nnz; e++) {
-            const uint32_t a = uf_find(par, row[e]), b = uf_find(par, col[e]);
-            if (a != b) par[std::max(a, b)] = std::min(a, b);
-        }
+        std::vector<uint32_t> root;
+        component_labels(n, nnz, row, col, root, st.s);
         std::vector<uint32_t> label(n), local(n), cid(n, ~0u);
         std::vector<std::vector<uint32_t>> members;
         for (uint32_t i = 0; i < n; i++) {
-            const uint32_t r = uf_find(par, i);
+            const uint32_t r = root[i];
             if (cid[r] == ~0u) {
                 cid[r] = (uint32_t)members.size();
                 members.emplace_back();
