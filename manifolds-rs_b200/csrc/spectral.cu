@@ -13,8 +13,12 @@
 // tridiagonal eigenproblem (at most 4 k + 30 rows) by cyclic Jacobi
 // rotations, the selection, and the placement of several components.
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <numeric>
+#include <thread>
 #include <vector>
 
 #include <cub/cub.cuh>
@@ -39,24 +43,35 @@ __global__ void k_spmv(uint32_t n, const uint64_t *__restrict__ ptr, const uint3
     if (lane == 0) y[row] = acc;
 }
 
-// out[j] = <V_j, w> for basis rows j < m: one block per row, fixed-order
-// block reduction
-__global__ void k_basis_dots(const double *__restrict__ V, uint32_t n, uint32_t m, const double *__restrict__ w,
-                             double *__restrict__ out)
+// Partial dot products for long vectors: block (b, j) sums a grid-strided
+// share of <V_j, w> into part[j * P + b]; k_sum_parts adds each row's P
+// partials in order (fixed order: deterministic).
+constexpr unsigned kParts = 64;
+
+__global__ void k_basis_dots_part(const double *__restrict__ V, uint32_t n, const double *__restrict__ w,
+                                  double *__restrict__ part)
 {
     __shared__ double sh[kBlk];
-    const uint32_t j = blockIdx.x;
-    if (j >= m) return;
+    const uint32_t j = blockIdx.y, b = blockIdx.x;
     const double *v = V + (size_t)j * n;
     double acc = 0.0;
-    for (uint32_t i = threadIdx.x; i < n; i += kBlk) acc += v[i] * w[i];
+    for (uint32_t i = b * kBlk + threadIdx.x; i < n; i += kParts * kBlk) acc += v[i] * w[i];
     sh[threadIdx.x] = acc;
     __syncthreads();
     for (int s = kBlk / 2; s > 0; s >>= 1) {
         if ((int)threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
         __syncthreads();
     }
-    if (threadIdx.x == 0) out[j] = sh[0];
+    if (threadIdx.x == 0) part[(size_t)j * kParts + b] = sh[0];
+}
+
+__global__ void k_sum_parts(const double *__restrict__ part, uint32_t m, double *__restrict__ out)
+{
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= m) return;
+    double acc = 0.0;
+    for (uint32_t b = 0; b < kParts; b++) acc += part[(size_t)j * kParts + b];
+    out[j] = acc;
 }
 
 // w -= sum_j c_j V_j (sub) or out = sum_j c_j V_j (!sub)
@@ -70,10 +85,23 @@ __global__ void k_basis_comb(const double *__restrict__ V, uint32_t n, uint32_t 
     w[i] = sub ? w[i] - acc : acc;
 }
 
-__global__ void k_scale(const double *__restrict__ x, uint32_t n, double s, double *__restrict__ dst)
+
+// dst = x / sqrt(*sq) (x unchanged when the norm is zero)
+__global__ void k_scale_by(const double *__restrict__ x, uint32_t n, const double *__restrict__ sq,
+                           double *__restrict__ dst)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) dst[i] = x[i] * s;
+    if (i >= n) return;
+    const double nr = sqrt(*sq);
+    dst[i] = nr > 0.0 ? x[i] / nr : x[i];
+}
+
+// c [0..j] = (0, ..., beta_{j-1}, alpha_j) from ab (alpha_i = ab[2i],
+// beta_i^2 = ab[2i + 1])
+__global__ void k_recurrence_coef(const double *__restrict__ ab, uint32_t j, double *__restrict__ c)
+{
+    for (uint32_t i = threadIdx.x; i <= j; i += blockDim.x)
+        c[i] = i == j ? ab[2 * j] : (i + 1 == j ? sqrt(ab[2 * i + 1]) : 0.0);
 }
 
 // Start vector: uniform in [-0.5, 0.5) from a counter-based SplitMix64
@@ -136,15 +164,14 @@ void jacobi_eigen(std::vector<double> &a, uint32_t m, std::vector<double> &evals
     for (uint32_t i = 0; i < m; i++) evals[i] = A(i, i);
 }
 
-double dev_dot(const double *a, const double *b, uint32_t n, double *d_tmp, cudaStream_t s)
+// out[j] = <V_j, w> for j < m
+void basis_dots(const double *V, uint32_t n, uint32_t m, const double *w, double *part, double *out, cudaStream_t s)
 {
-    k_basis_dots<<<1, kBlk, 0, s>>>(a, n, 1, b, d_tmp);
-    check_launch("k_basis_dots");
-    double h = 0.0;
-    d2h(&h, d_tmp, 1, s);
-    sync(s);
-    return h;
+    k_basis_dots_part<<<dim3(kParts, m), kBlk, 0, s>>>(V, n, w, part);
+    k_sum_parts<<<ceil_div(m, 128), 128, 0, s>>>(part, m, out);
+    check_launch("basis dots");
 }
+
 
 }  // namespace
 
@@ -161,42 +188,43 @@ void smallest_eigenpairs_dev(uint32_t n, const uint64_t *d_ptr, const uint32_t *
 {
     if (n == 0) fail(UMAPCU_NO_DATA, "eigenpairs of an empty matrix");
     const uint32_t n_iter = std::min<uint32_t>(n_components * 4 + 30, n);
-    DevBuf<double> V((size_t)n_iter * n, s), w(n, s), c(n_iter, s), tmp(1, s);
+    // The recurrence runs without host round trips: alpha_j and beta_j stay
+    // in device memory (ab[2j], ab[2j + 1] = beta_j^2) and are read back once
+    // at the end; a breakdown (beta < 1e-12) truncates the steps there, so
+    // whatever the later steps computed is discarded.
+    DevBuf<double> V((size_t)n_iter * n, s), w(n, s), c(n_iter, s), ab(2 * (size_t)n_iter + 2, s),
+        part((size_t)n_iter * kParts, s);
     const unsigned g = ceil_div(n, kBlk);
     k_random_start<<<g, kBlk, 0, s>>>(V.p, n, seed);
-    check_launch("k_random_start");
-    {
-        const double nr = std::sqrt(dev_dot(V.p, V.p, n, tmp.p, s));
-        k_scale<<<g, kBlk, 0, s>>>(V.p, n, nr > 0 ? 1.0 / nr : 1.0, V.p);
-    }
-    std::vector<double> alpha, beta, hc(n_iter);
-    uint32_t n_done = 0;
+    basis_dots(V.p, n, 1, V.p, part.p, ab.p + 2 * n_iter, s);  // |v0|^2
+    k_scale_by<<<g, kBlk, 0, s>>>(V.p, n, ab.p + 2 * n_iter, V.p);
+    check_launch("start vector");
     for (uint32_t j = 0; j < n_iter; j++) {
         double *vj = V.p + (size_t)j * n;
-        n_done = j + 1;
         k_spmv<<<ceil_div((uint64_t)n * 32, kBlk), kBlk, 0, s>>>(n, d_ptr, d_col, d_val, vj, w.p);
-        check_launch("k_spmv");
-        const double a = dev_dot(w.p, vj, n, tmp.p, s);
-        alpha.push_back(a);
-        // w -= alpha v_j + beta_{j-1} v_{j-1}
-        std::fill(hc.begin(), hc.end(), 0.0);
-        hc[j] = a;
-        if (j) hc[j - 1] = beta[j - 1];
-        h2d(c.p, hc.data(), j + 1, s);
+        basis_dots(vj, n, 1, w.p, part.p, ab.p + 2 * j, s);  // alpha_j
+        // w -= alpha_j v_j + beta_{j-1} v_{j-1}
+        k_recurrence_coef<<<1, 32, 0, s>>>(ab.p, j, c.p);
         k_basis_comb<<<g, kBlk, 0, s>>>(V.p, n, j + 1, c.p, w.p, true);
         // full reorthogonalisation: two classical Gram-Schmidt passes
         for (int pass = 0; pass < 2; pass++) {
-            k_basis_dots<<<j + 1, kBlk, 0, s>>>(V.p, n, j + 1, w.p, c.p);
+            basis_dots(V.p, n, j + 1, w.p, part.p, c.p, s);
             k_basis_comb<<<g, kBlk, 0, s>>>(V.p, n, j + 1, c.p, w.p, true);
         }
-        check_launch("reorthogonalise");
-        const double b = std::sqrt(dev_dot(w.p, w.p, n, tmp.p, s));
-        beta.push_back(b);
-        if (b < 1e-12) break;
-        if (j + 1 < n_iter) {
-            k_scale<<<g, kBlk, 0, s>>>(w.p, n, 1.0 / b, V.p + (size_t)(j + 1) * n);
-            check_launch("k_scale");
-        }
+        basis_dots(w.p, n, 1, w.p, part.p, ab.p + 2 * j + 1, s);  // beta_j^2
+        if (j + 1 < n_iter) k_scale_by<<<g, kBlk, 0, s>>>(w.p, n, ab.p + 2 * j + 1, V.p + (size_t)(j + 1) * n);
+        check_launch("lanczos step");
+    }
+    std::vector<double> hab(2 * (size_t)n_iter);
+    d2h(hab.data(), ab.p, 2 * (size_t)n_iter, s);
+    sync(s);
+    std::vector<double> alpha, beta;
+    uint32_t n_done = 0;
+    for (uint32_t j = 0; j < n_iter; j++) {
+        alpha.push_back(hab[2 * j]);
+        beta.push_back(std::sqrt(std::max(0.0, hab[2 * j + 1])));
+        n_done = j + 1;
+        if (beta.back() < 1e-12) break;
     }
     const uint32_t m = n_done;
     std::vector<double> T((size_t)m * m, 0.0), tev, tvec;
@@ -482,6 +510,7 @@ umapcu_status umapcu_smallest_eigenpairs(uint32_t n, const uint64_t *ptr, const 
             if (ptr[i + 1] < ptr[i]) return UMAPCU_BAD_ARG;
         for (uint64_t e = 0; e < nnz; e++)
             if (col[e] >= n) return UMAPCU_BAD_ARG;
+        keep_pool_memory();
         Stream st;
         DevBuf<uint64_t> dp(n + 1, st.s);
         DevBuf<uint32_t> dc(nnz ? nnz : 1, st.s);
@@ -508,11 +537,24 @@ umapcu_status umapcu_spectral_layout(const uint32_t *row, const uint32_t *col, c
         for (uint64_t e = 0; e < nnz; e++)
             if (row[e] >= n || col[e] >= n) return UMAPCU_BAD_ARG;
         const double rng = range > 0.0f ? (double)range : 10.0;  // SPECTRAL_RANGE, init.rs:17
+        keep_pool_memory();
         Stream st;
+        const bool timing = getenv("UMAPCU_TIMING") != nullptr;
+        auto t0 = std::chrono::steady_clock::now();
+        auto lap = [&](const char *what) {
+            if (!timing) return;
+            sync(st.s);
+            auto t1 = std::chrono::steady_clock::now();
+            fprintf(stderr, "umapcu timing: spectral %-12s %9.3f ms\n", what,
+                    std::chrono::duration<double, std::milli>(t1 - t0).count());
+            t0 = t1;
+        };
+        lap("validate");
         // connected components (find_connected_components, init.rs:349-391),
         // labelled in order of their smallest point, members ascending
         std::vector<uint32_t> root;
         component_labels(n, nnz, row, col, root, st.s);
+        lap("components");
         std::vector<uint32_t> label(n), local(n), cid(n, ~0u);
         std::vector<std::vector<uint32_t>> members;
         for (uint32_t i = 0; i < n; i++) {
@@ -530,6 +572,7 @@ umapcu_status umapcu_spectral_layout(const uint32_t *row, const uint32_t *col, c
             // single_component_spectral + finalise_spectral_embedding
             // (init.rs:876-958): centre, scale to range, N(0, 1e-4) noise
             component_raw(n, nnz, row, col, val, n_comp, seed, out, st.s);
+            lap("eigen");
             centre_and_scale(out, n, n_comp, rng);
             Mix r{seed + 9999};
             for (double &x : out) x += 1e-4 * r.normal();
@@ -564,6 +607,39 @@ umapcu_status umapcu_spectral_layout(const uint32_t *row, const uint32_t *col, c
                 sc[q] = local[col[e]];
                 sw[q] = val[e];
             }
+            // the components' eigen-solves are independent: a few host
+            // threads, one stream each, largest components first
+            std::vector<std::vector<double>> subs(C);
+            std::vector<uint32_t> big;
+            for (uint32_t c = 0; c < C; c++)
+                if (members[c].size() >= 2 * n_comp) big.push_back(c);
+            std::stable_sort(big.begin(), big.end(),
+                             [&](uint32_t a, uint32_t b) { return members[a].size() > members[b].size(); });
+            std::atomic<size_t> next{0};
+            std::vector<umapcu_status> errs(std::min<size_t>(8, big.size()), UMAPCU_OK);
+            std::vector<std::thread> pool;
+            int dev = 0;
+            check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+            for (size_t t = 0; t < errs.size(); t++)
+                pool.emplace_back([&, t]() {
+                    try {
+                        check_cuda(cudaSetDevice(dev), "cudaSetDevice");
+                        Stream ts;
+                        for (size_t q; (q = next.fetch_add(1)) < big.size();) {
+                            const uint32_t c = big[q];
+                            component_raw((uint32_t)members[c].size(), cnt[c + 1] - cnt[c], sr.data() + cnt[c],
+                                          sc.data() + cnt[c], sw.data() + cnt[c], n_comp, seed + c, subs[c], ts.s);
+                        }
+                    } catch (const Error &e) {
+                        errs[t] = e.status;
+                    } catch (...) {
+                        errs[t] = UMAPCU_CUDA_LAUNCH;
+                    }
+                });
+            for (auto &th : pool) th.join();
+            for (umapcu_status e : errs)
+                if (e != UMAPCU_OK) return e;
+            lap("eigen");
             Mix r{seed};
             for (uint32_t c = 0; c < C; c++) {
                 const double *cen = meta.data() + (size_t)c * n_comp;
@@ -585,9 +661,7 @@ umapcu_status umapcu_spectral_layout(const uint32_t *row, const uint32_t *col, c
                             out[(size_t)gi * n_comp + d] = cen[d] + (2.0 * r.uniform() - 1.0) * dr;
                     continue;
                 }
-                std::vector<double> sub;
-                component_raw(nc, cnt[c + 1] - cnt[c], sr.data() + cnt[c], sc.data() + cnt[c], sw.data() + cnt[c],
-                              n_comp, seed + c, sub, st.s);
+                const std::vector<double> &sub = subs[c];
                 const double sm = max_abs(sub);
                 const double ex = sm > 1e-8 ? dr / sm : 1.0;
                 for (uint32_t li = 0; li < nc; li++)
@@ -597,6 +671,7 @@ umapcu_status umapcu_spectral_layout(const uint32_t *row, const uint32_t *col, c
             centre_and_scale(out, n, n_comp, rng);
         }
         for (size_t i = 0; i < out.size(); i++) embd[i] = (float)out[i];
+        lap("finish");
         return UMAPCU_OK;
     });
 }
