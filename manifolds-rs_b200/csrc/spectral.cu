@@ -5,13 +5,16 @@
 // negative normalised adjacency -D^-1/2 A D^-1/2 per connected component,
 // eigenvectors 1..n_comp, centred, scaled to a range, small noise).
 //
-// Device side: CSR SpMV in f64, dot products, the two-pass classical
+// Device side: the normalised adjacency (stable row sort, per-row degree
+// sums), connected components (label hooking with pointer jumping), CSR SpMV
+// in f64, dot products (fixed-order partial sums), the two-pass classical
 // Gram-Schmidt against the whole Krylov basis (basis^T w, then w -= basis c,
-// twice: one pass over the basis each way instead of the reference's
-// sequential modified Gram-Schmidt; both keep the basis orthogonal to
-// rounding), the back-transformation basis * c. Host side: the small
-// tridiagonal eigenproblem (at most 4 k + 30 rows) by cyclic Jacobi
-// rotations, the selection, and the placement of several components.
+// twice, in place of the reference's sequential modified Gram-Schmidt; both
+// keep the basis orthogonal to rounding), the back-transformation basis * c;
+// alpha and beta stay on the device until the recurrence ends. Host side:
+// the small tridiagonal eigenproblem (at most 4 k + 30 rows) by cyclic Jacobi
+// rotations, the selection, and the placement of several components (their
+// eigen-solves run concurrently, one host thread and stream each).
 #include <algorithm>
 #include <atomic>
 #include <chrono>
