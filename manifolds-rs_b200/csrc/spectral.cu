@@ -13,15 +13,16 @@
 // keep the basis orthogonal to rounding), the back-transformation basis * c;
 // alpha and beta stay on the device until the recurrence ends. Host side:
 // the small tridiagonal eigenproblem (at most 4 k + 30 rows) by cyclic Jacobi
-// rotations, the selection, and the placement of several components (their
-// eigen-solves run concurrently, one host thread and stream each).
+// rotations, the selection, and the placement of several components. The
+// components of a graph are solved together: one Lanczos over the
+// block-diagonal whole-graph matrix in which every dot product, recurrence
+// coefficient, breakdown test and back-transformation is per component, so
+// thirty components cost about as many launches as one.
 #include <algorithm>
-#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdlib>
 #include <numeric>
-#include <thread>
 #include <vector>
 
 #include <cub/cub.cuh>
@@ -307,6 +308,126 @@ __global__ void k_neg_norm_values(uint32_t n, const uint64_t *__restrict__ ptr, 
     }
 }
 
+// ---- batched Lanczos: every component's recurrence advances together.
+// The normalised adjacency of the whole graph is block-diagonal (no edge
+// crosses components), so one SpMV serves all of them; the per-component
+// dot products run over each component's member list (mem[seg[s] ..
+// seg[s + 1]]) as fixed-order partial sums; sidx[g] is point g's segment
+// (~0: not solved, its vector entries stay zero).
+// Per-component dot products over the whole index space: every component
+// (segment) is cut into chunks of at most kSegChunk of its members, one block
+// per (chunk, row); a segment's chunks are consecutive work items
+// [pofs[s], pofs[s + 1]) and are summed in order, so the result does not
+// depend on scheduling.
+constexpr uint32_t kSegChunk = 4096;
+
+// part[r * n_items + t] = <V_r, w> over work item t's members
+__global__ void k_seg_dots_part(const double *__restrict__ V, uint64_t n, const double *__restrict__ w,
+                                const uint32_t *__restrict__ mem, const uint32_t *__restrict__ item_beg,
+                                const uint32_t *__restrict__ item_end, uint32_t n_items, double *__restrict__ part)
+{
+    __shared__ double sh[kBlk];
+    const uint32_t t = blockIdx.x, r = blockIdx.y;
+    const double *v = V + (size_t)r * n;
+    double acc = 0.0;
+    for (uint32_t i = item_beg[t] + threadIdx.x; i < item_end[t]; i += kBlk) {
+        const uint32_t g = mem[i];
+        acc += v[g] * w[g];
+    }
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int h = kBlk / 2; h > 0; h >>= 1) {
+        if ((int)threadIdx.x < h) sh[threadIdx.x] += sh[threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[(size_t)r * n_items + t] = sh[0];
+}
+
+// out[r * S + s] = sum of segment s's work items of row r, in order
+__global__ void k_seg_sum_parts(const double *__restrict__ part, uint32_t n_items, const uint32_t *__restrict__ pofs,
+                                uint32_t S, uint32_t rows, double *__restrict__ out)
+{
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (uint64_t)rows * S) return;
+    const uint32_t r = (uint32_t)(t / S), sg = (uint32_t)(t - (uint64_t)r * S);
+    double acc = 0.0;
+    for (uint32_t q = pofs[sg]; q < pofs[sg + 1]; q++) acc += part[(size_t)r * n_items + q];
+    out[t] = acc;
+}
+
+// w[g] -= sum_{r < m} c[r * S + s] V_r[g] (sub), or w[g] = that sum, for the
+// points of solved segments
+__global__ void k_seg_comb(const double *__restrict__ V, uint64_t n, uint32_t m, const double *__restrict__ c,
+                           uint32_t S, const uint32_t *__restrict__ sidx, double *__restrict__ w, bool sub)
+{
+    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    const uint32_t sg = sidx[g];
+    if (sg == ~0u) return;
+    double acc = 0.0;
+    for (uint32_t r = 0; r < m; r++) acc += c[(size_t)r * S + sg] * V[(size_t)r * n + g];
+    w[g] = sub ? w[g] - acc : acc;
+}
+
+// recurrence coefficients of step j: c[r][s] = alpha_j(s) at r = j,
+// beta_{j-1}(s) at r = j - 1, else 0; ab = [step][2][S] (alpha, beta^2)
+__global__ void k_seg_recurrence(const double *__restrict__ ab, uint32_t j, uint32_t S, double *__restrict__ c)
+{
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (j + 1) * S) return;
+    const uint32_t r = t / S, sg = t - r * S;
+    double v = 0.0;
+    if (r == j) v = ab[((size_t)j * 2) * S + sg];
+    else if (r + 1 == j) v = sqrt(ab[((size_t)r * 2 + 1) * S + sg]);
+    c[t] = v;
+}
+
+// v_{j+1}[g] = w[g] / beta_j(s) while segment s still steps (j + 1 < its
+// step count and no breakdown so far), else 0
+__global__ void k_seg_next(const double *__restrict__ w, uint64_t n, const uint32_t *__restrict__ sidx,
+                           const double *__restrict__ ab, uint32_t j, uint32_t S, const uint32_t *__restrict__ iters,
+                           double *__restrict__ vnext)
+{
+    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    const uint32_t sg = sidx[g];
+    if (sg == ~0u) return;
+    bool live = j + 1 < iters[sg];
+    for (uint32_t r = 0; live && r <= j; r++) live = sqrt(ab[((size_t)r * 2 + 1) * S + sg]) >= 1e-12;
+    vnext[g] = live ? w[g] / sqrt(ab[((size_t)j * 2 + 1) * S + sg]) : 0.0;
+}
+
+// start vectors: point g with local index l in component `label` gets the
+// same value k_random_start gives index l under seed + label; then scaled by
+// its segment's norm (sq = squared norms per segment)
+__global__ void k_seg_start(uint64_t n, const uint32_t *__restrict__ sidx, const uint32_t *__restrict__ lidx,
+                            const uint32_t *__restrict__ seg_label, uint64_t seed, double *__restrict__ v)
+{
+    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    const uint32_t sg = sidx[g];
+    if (sg == ~0u) {
+        v[g] = 0.0;
+        return;
+    }
+    uint64_t z = (seed + seg_label[sg]) + 0x9E3779B97F4A7C15ull * (uint64_t)(lidx[g] + 1);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    v[g] = (double)(z >> 11) * (1.0 / 9007199254740992.0) - 0.5;
+}
+
+__global__ void k_seg_scale(double *__restrict__ v, uint64_t n, const uint32_t *__restrict__ sidx,
+                            const double *__restrict__ sq)
+{
+    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    const uint32_t sg = sidx[g];
+    if (sg == ~0u) return;
+    const double nr = sqrt(sq[sg]);
+    if (nr > 0.0) v[g] /= nr;
+}
+
 // -D^-1/2 A D^-1/2 of a COO graph on n nodes (graph_to_negative_normalised_
 // adjacency, src/data/init.rs:210-256) built on the device: degrees include
 // self loops, self-loop entries carry 0 (the reference drops them), CSR rows
@@ -424,31 +545,135 @@ struct Mix {
     }
 };
 
-// single_component_spectral_raw (src/data/init.rs:276-320): eigenvectors
-// 1..n_comp of the component's -D^-1/2 A D^-1/2; graphs of at most n_comp + 1
-// points and dimensions Lanczos did not supply are uniform in [-1, 1).
-void component_raw(uint32_t n, uint64_t nnz, const uint32_t *row, const uint32_t *col, const float *w,
-                   uint32_t n_comp, uint64_t seed, std::vector<double> &out, cudaStream_t s)
+// single_component_spectral_raw (src/data/init.rs:276-320) for every
+// component in `solve` at once (batched Lanczos, see above): raw[c] [n_c *
+// n_comp] = eigenvectors 1..n_comp of the component's -D^-1/2 A D^-1/2
+// (dimensions Lanczos did not supply: uniform in [-1, 1)), each component
+// from its own start vector (seed + label). members[c] ascending.
+void batched_component_raw(uint32_t n, const DevBuf<uint64_t> &ptr, const DevBuf<uint32_t> &ci,
+                           const DevBuf<double> &val, const std::vector<std::vector<uint32_t>> &members,
+                           const std::vector<uint32_t> &solve, uint32_t n_comp, uint64_t seed,
+                           std::vector<std::vector<double>> &raw, cudaStream_t s)
 {
-    out.assign((size_t)n * n_comp, 0.0);
-    if (n <= n_comp + 1) {
-        Mix r{seed};
-        for (double &v : out) v = 2.0 * r.uniform() - 1.0;
-        return;
+    const uint32_t S = (uint32_t)solve.size();
+    if (!S) return;
+    const uint32_t kk = n_comp + 1;
+    std::vector<uint32_t> hmem, hsidx(n, ~0u), hlidx(n, 0), hlabel(S), hiters(S), hbeg, hend, hpofs(S + 1, 0);
+    uint32_t it_max = 0;
+    for (uint32_t q = 0; q < S; q++) {
+        const std::vector<uint32_t> &mem = members[solve[q]];
+        const uint32_t at = (uint32_t)hmem.size();
+        for (uint32_t l = 0; l < mem.size(); l++) {
+            hsidx[mem[l]] = q;
+            hlidx[mem[l]] = l;
+            hmem.push_back(mem[l]);
+        }
+        for (uint32_t b = 0; b < mem.size(); b += kSegChunk) {
+            hbeg.push_back(at + b);
+            hend.push_back(at + std::min<uint32_t>(b + kSegChunk, (uint32_t)mem.size()));
+        }
+        hpofs[q + 1] = (uint32_t)hbeg.size();
+        hlabel[q] = solve[q];
+        hiters[q] = std::min<uint32_t>(kk * 4 + 30, (uint32_t)mem.size());
+        it_max = std::max(it_max, hiters[q]);
     }
-    DevBuf<uint64_t> ptr;
-    DevBuf<uint32_t> ci;
-    DevBuf<double> val;
-    neg_normalised_adjacency(n, nnz, row, col, w, ptr, ci, val, s);
-    std::vector<float> ev, vec;
-    uint32_t k = 0;
-    smallest_eigenpairs_dev(n, ptr.p, ci.p, val.p, std::min(n_comp + 1, n), seed, ev, vec, k, s);
-    for (uint32_t d = 0; d < n_comp; d++) {
-        if (d + 1 < k) {
-            for (uint32_t i = 0; i < n; i++) out[(size_t)i * n_comp + d] = vec[(size_t)i * k + d + 1];
-        } else {
-            Mix r{seed + d};
-            for (uint32_t i = 0; i < n; i++) out[(size_t)i * n_comp + d] = 2.0 * r.uniform() - 1.0;
+    const uint32_t n_items = (uint32_t)hbeg.size();
+    DevBuf<uint32_t> mem(hmem.size(), s), ibeg(n_items, s), iend(n_items, s), pofs(S + 1, s), sidx(n, s), lidx(n, s),
+        label(S, s), iters(S, s);
+    h2d(mem.p, hmem.data(), hmem.size(), s);
+    h2d(ibeg.p, hbeg.data(), n_items, s);
+    h2d(iend.p, hend.data(), n_items, s);
+    h2d(pofs.p, hpofs.data(), S + 1, s);
+    h2d(sidx.p, hsidx.data(), n, s);
+    h2d(lidx.p, hlidx.data(), n, s);
+    h2d(label.p, hlabel.data(), S, s);
+    h2d(iters.p, hiters.data(), S, s);
+    DevBuf<double> V((size_t)it_max * n, s), w(n, s), c((size_t)it_max * S, s), ab((size_t)it_max * 2 * S, s),
+        part((size_t)it_max * n_items, s), sq(S, s);
+    check_cuda(cudaMemsetAsync(V.p, 0, sizeof(double) * V.n, s), "memset");  // rows of unsolved points stay 0
+    const unsigned g = ceil_div(n, kBlk);
+    auto seg_dots = [&](const double *Vrows, uint32_t rows, const double *x, double *out) {
+        k_seg_dots_part<<<dim3(n_items, rows), kBlk, 0, s>>>(Vrows, n, x, mem.p, ibeg.p, iend.p, n_items, part.p);
+        k_seg_sum_parts<<<ceil_div((uint64_t)rows * S, 128), 128, 0, s>>>(part.p, n_items, pofs.p, S, rows, out);
+    };
+    k_seg_start<<<g, kBlk, 0, s>>>(n, sidx.p, lidx.p, label.p, seed, V.p);
+    seg_dots(V.p, 1, V.p, sq.p);
+    k_seg_scale<<<g, kBlk, 0, s>>>(V.p, n, sidx.p, sq.p);
+    check_launch("batched start");
+    for (uint32_t j = 0; j < it_max; j++) {
+        const double *vj = V.p + (size_t)j * n;
+        k_spmv<<<ceil_div((uint64_t)n * 32, kBlk), kBlk, 0, s>>>(n, ptr.p, ci.p, val.p, vj, w.p);
+        seg_dots(vj, 1, w.p, ab.p + (size_t)j * 2 * S);  // alpha_j per segment
+        k_seg_recurrence<<<ceil_div((uint64_t)(j + 1) * S, 128), 128, 0, s>>>(ab.p, j, S, c.p);
+        k_seg_comb<<<g, kBlk, 0, s>>>(V.p, n, j + 1, c.p, S, sidx.p, w.p, true);
+        for (int pass = 0; pass < 2; pass++) {
+            seg_dots(V.p, j + 1, w.p, c.p);
+            k_seg_comb<<<g, kBlk, 0, s>>>(V.p, n, j + 1, c.p, S, sidx.p, w.p, true);
+        }
+        seg_dots(w.p, 1, w.p, ab.p + ((size_t)j * 2 + 1) * S);  // beta_j^2
+        if (j + 1 < it_max)
+            k_seg_next<<<g, kBlk, 0, s>>>(w.p, n, sidx.p, ab.p, j, S, iters.p, V.p + (size_t)(j + 1) * n);
+        check_launch("batched lanczos step");
+    }
+    std::vector<double> hab((size_t)it_max * 2 * S);
+    d2h(hab.data(), ab.p, hab.size(), s);
+    sync(s);
+    // per component: truncate, tridiagonal eigenproblem; keep the Ritz
+    // coefficients of its kk smallest eigenvalues (ritz[q] [e][m_q])
+    std::vector<std::vector<double>> ritz(S);
+    std::vector<uint32_t> found(S), msteps(S);
+    for (uint32_t q = 0; q < S; q++) {
+        std::vector<double> alpha, beta;
+        for (uint32_t j = 0; j < hiters[q]; j++) {
+            alpha.push_back(hab[((size_t)j * 2) * S + q]);
+            beta.push_back(std::sqrt(std::max(0.0, hab[((size_t)j * 2 + 1) * S + q])));
+            if (beta.back() < 1e-12) break;
+        }
+        const uint32_t m = (uint32_t)alpha.size();
+        std::vector<double> T((size_t)m * m, 0.0), tev, tvec;
+        for (uint32_t i = 0; i < m; i++) {
+            T[(size_t)i * m + i] = alpha[i];
+            if (i + 1 < m) T[(size_t)i * m + i + 1] = T[(size_t)(i + 1) * m + i] = beta[i];
+        }
+        jacobi_eigen(T, m, tev, tvec);
+        std::vector<uint32_t> order(m);
+        std::iota(order.begin(), order.end(), 0u);
+        std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return tev[x] < tev[y]; });
+        found[q] = std::min(kk, m);
+        msteps[q] = m;
+        ritz[q].resize((size_t)found[q] * m);
+        for (uint32_t e = 0; e < found[q]; e++)
+            std::copy(tvec.begin() + (size_t)order[e] * m, tvec.begin() + (size_t)(order[e] + 1) * m,
+                      ritz[q].begin() + (size_t)e * m);
+    }
+    // back-transform eigenvector e of every component, normalise per component
+    for (uint32_t q = 0; q < S; q++) raw[solve[q]].assign(members[solve[q]].size() * n_comp, 0.0);
+    std::vector<double> hv(n), hn(S), coef((size_t)it_max * S);
+    for (uint32_t e = 1; e < kk; e++) {
+        std::fill(coef.begin(), coef.end(), 0.0);  // [r][s]
+        for (uint32_t q = 0; q < S; q++)
+            if (e < found[q])
+                for (uint32_t r = 0; r < msteps[q]; r++)
+                    coef[(size_t)r * S + q] = ritz[q][(size_t)e * msteps[q] + r];
+        h2d(c.p, coef.data(), coef.size(), s);
+        k_seg_comb<<<g, kBlk, 0, s>>>(V.p, n, it_max, c.p, S, sidx.p, w.p, false);
+        seg_dots(w.p, 1, w.p, sq.p);
+        check_launch("batched back-transform");
+        d2h(hv.data(), w.p, n, s);
+        d2h(hn.data(), sq.p, S, s);
+        sync(s);
+        const uint32_t d = e - 1;
+        for (uint32_t q = 0; q < S; q++) {
+            const std::vector<uint32_t> &mem = members[solve[q]];
+            std::vector<double> &out = raw[solve[q]];
+            if (e < found[q]) {
+                const double nr = std::sqrt(hn[q]);
+                for (uint32_t l = 0; l < mem.size(); l++)
+                    out[(size_t)l * n_comp + d] = (double)(float)(nr > 0 ? hv[mem[l]] / nr : hv[mem[l]]);
+            } else {
+                Mix r{seed + solve[q] + d};
+                for (uint32_t l = 0; l < mem.size(); l++) out[(size_t)l * n_comp + d] = 2.0 * r.uniform() - 1.0;
+            }
         }
     }
 }
@@ -558,7 +783,7 @@ umapcu_status umapcu_spectral_layout(const uint32_t *row, const uint32_t *col, c
         std::vector<uint32_t> root;
         component_labels(n, nnz, row, col, root, st.s);
         lap("components");
-        std::vector<uint32_t> label(n), local(n), cid(n, ~0u);
+        std::vector<uint32_t> cid(n, ~0u);
         std::vector<std::vector<uint32_t>> members;
         for (uint32_t i = 0; i < n; i++) {
             const uint32_t r = root[i];
@@ -566,15 +791,24 @@ umapcu_status umapcu_spectral_layout(const uint32_t *row, const uint32_t *col, c
                 cid[r] = (uint32_t)members.size();
                 members.emplace_back();
             }
-            label[i] = cid[r];
-            local[i] = (uint32_t)members[label[i]].size();
-            members[label[i]].push_back(i);
+            members[cid[r]].push_back(i);
         }
         std::vector<double> out((size_t)n * n_comp, 0.0);
         if (members.size() == 1) {
             // single_component_spectral + finalise_spectral_embedding
             // (init.rs:876-958): centre, scale to range, N(0, 1e-4) noise
-            component_raw(n, nnz, row, col, val, n_comp, seed, out, st.s);
+            if (n <= n_comp + 1) {
+                Mix r{seed};
+                for (double &v : out) v = 2.0 * r.uniform() - 1.0;
+            } else {
+                DevBuf<uint64_t> ptr;
+                DevBuf<uint32_t> ci;
+                DevBuf<double> av;
+                neg_normalised_adjacency(n, nnz, row, col, val, ptr, ci, av, st.s);
+                std::vector<std::vector<double>> raw(1);
+                batched_component_raw(n, ptr, ci, av, members, {0u}, n_comp, seed, raw, st.s);
+                out.swap(raw[0]);
+            }
             lap("eigen");
             centre_and_scale(out, n, n_comp, rng);
             Mix r{seed + 9999};
@@ -594,54 +828,34 @@ umapcu_status umapcu_spectral_layout(const uint32_t *row, const uint32_t *col, c
             const double mm = max_abs(meta);
             if (mm > 1e-8)
                 for (double &x : meta) x /= mm;
-            std::vector<uint64_t> cnt(C + 1, 0);
-            for (uint64_t e = 0; e < nnz; e++)
-                if (label[row[e]] == label[col[e]]) cnt[label[row[e]] + 1]++;
-            for (uint32_t c = 0; c < C; c++) cnt[c + 1] += cnt[c];
-            const size_t m = cnt[C] ? cnt[C] : 1;
-            std::vector<uint32_t> sr(m), sc(m);
-            std::vector<float> sw(m);
-            std::vector<uint64_t> at(cnt.begin(), cnt.end() - 1);
-            for (uint64_t e = 0; e < nnz; e++) {
-                const uint32_t c = label[row[e]];
-                if (c != label[col[e]]) continue;
-                const uint64_t q = at[c]++;
-                sr[q] = local[row[e]];
-                sc[q] = local[col[e]];
-                sw[q] = val[e];
-            }
-            // the components' eigen-solves are independent: a few host
-            // threads, one stream each, largest components first
+            // the components' eigen-solves advance together: one Lanczos
+            // over the block-diagonal whole-graph matrix, every operation
+            // per component (batched_component_raw), in batches of at most
+            // 16384 components
             std::vector<std::vector<double>> subs(C);
-            std::vector<uint32_t> big;
-            for (uint32_t c = 0; c < C; c++)
-                if (members[c].size() >= 2 * n_comp) big.push_back(c);
-            std::stable_sort(big.begin(), big.end(),
-                             [&](uint32_t a, uint32_t b) { return members[a].size() > members[b].size(); });
-            std::atomic<size_t> next{0};
-            std::vector<umapcu_status> errs(std::min<size_t>(8, big.size()), UMAPCU_OK);
-            std::vector<std::thread> pool;
-            int dev = 0;
-            check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
-            for (size_t t = 0; t < errs.size(); t++)
-                pool.emplace_back([&, t]() {
-                    try {
-                        check_cuda(cudaSetDevice(dev), "cudaSetDevice");
-                        Stream ts;
-                        for (size_t q; (q = next.fetch_add(1)) < big.size();) {
-                            const uint32_t c = big[q];
-                            component_raw((uint32_t)members[c].size(), cnt[c + 1] - cnt[c], sr.data() + cnt[c],
-                                          sc.data() + cnt[c], sw.data() + cnt[c], n_comp, seed + c, subs[c], ts.s);
-                        }
-                    } catch (const Error &e) {
-                        errs[t] = e.status;
-                    } catch (...) {
-                        errs[t] = UMAPCU_CUDA_LAUNCH;
-                    }
-                });
-            for (auto &th : pool) th.join();
-            for (umapcu_status e : errs)
-                if (e != UMAPCU_OK) return e;
+            std::vector<uint32_t> solve;
+            for (uint32_t c = 0; c < C; c++) {
+                const uint32_t nc = (uint32_t)members[c].size();
+                if (nc < 2 * n_comp) continue;
+                if (nc > n_comp + 1) {
+                    solve.push_back(c);
+                } else {  // too small for Lanczos (single_component_spectral_raw)
+                    Mix r{seed + c};
+                    subs[c].resize((size_t)nc * n_comp);
+                    for (double &v : subs[c]) v = 2.0 * r.uniform() - 1.0;
+                }
+            }
+            if (!solve.empty()) {
+                DevBuf<uint64_t> ptr;
+                DevBuf<uint32_t> ci;
+                DevBuf<double> av;
+                neg_normalised_adjacency(n, nnz, row, col, val, ptr, ci, av, st.s);
+                for (size_t b = 0; b < solve.size(); b += 16384) {
+                    const std::vector<uint32_t> part(solve.begin() + b,
+                                                     solve.begin() + std::min(solve.size(), b + 16384));
+                    batched_component_raw(n, ptr, ci, av, members, part, n_comp, seed, subs, st.s);
+                }
+            }
             lap("eigen");
             Mix r{seed};
             for (uint32_t c = 0; c < C; c++) {

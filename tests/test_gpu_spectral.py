@@ -128,3 +128,34 @@ def test_spectral_layout_several_components():
     assert np.isfinite(y).all() and abs(np.abs(y).max() - 10.0) < 1e-3
     a, b = y[:800].mean(0), y[800:].mean(0)
     assert np.linalg.norm(a - b) > 5.0 and abs(a[1] - b[1]) < 1.0
+
+
+def test_spectral_layout_components_solved_together_match_oracle():
+    """Three components of different sizes (two strips and a 5-point chain)
+    go through one batched Lanczos; each strip's placed coordinates must be an
+    affine image of the oracle's eigenvectors of that component alone, run
+    from the component's own start vector (seed + its label)."""
+    from oracle import oracle as O
+    sizes = (900, 600)
+    parts, off = [], 0
+    for i, m in enumerate(sizes):
+        g = _strip_graph(m, seed=11 + i)
+        parts.append((g["row"] + off, g["col"] + off, g["val"]))
+        off += m
+    chain = np.arange(off, off + 4, dtype=np.uint32)           # 5 points, too small to solve
+    parts.append((np.concatenate([chain, chain + 1]), np.concatenate([chain + 1, chain]), np.ones(8, np.float32)))
+    n = off + 5
+    r, c, v = (np.concatenate([p[k] for p in parts]) for k in range(3))
+    coo = umapcu.CoordinateList(r.astype(np.uint32), c.astype(np.uint32), v.astype(np.float32), n)
+    seed = 4
+    y = umapcu.spectral_layout(coo, 2, seed=seed)
+    assert y.shape == (n, 2) and np.isfinite(y).all() and abs(np.abs(y).max() - 10.0) < 1e-3
+    off = 0
+    for label, m in enumerate(sizes):
+        sl = slice(off, off + m)
+        sub = dict(row=parts[label][0] - off, col=parts[label][1] - off, val=parts[label][2])
+        _, V = O.lanczos_smallest(_neg_norm_adjacency(sub, m), 3, O.splitmix_start(m, seed + label))
+        for d in range(2):
+            corr = np.corrcoef(V[:, 1 + d], y[sl, d])[0, 1]
+            assert abs(corr) > 0.9999, (label, d, corr)
+        off += m
