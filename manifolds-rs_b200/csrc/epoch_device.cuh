@@ -214,28 +214,25 @@ __device__ __forceinline__ uint32_t local_node(const uint32_t *beg, uint32_t p)
     return j;
 }
 
-// One batch of `cnt` queued active entries (cnt <= 32) starting at queue
-// slot q0; lane t = slot q0 + t. The lane's node is found here (active
-// entries only), and the other endpoint's row and the first chunk of
-// negatives' rows are gathered together, so a batch waits on L2 once.
+// One batch of up to 32 active entries, lane t = entry t (`live` lanes
+// only): CSR position p, other endpoint o, the entry's node as an index j
+// into the segment, and its offset el within the node's row. The other
+// endpoint's row and the first chunk of negatives' rows are gathered
+// together, so a batch waits on L2 once.
 // FAST: the common configuration resolved at compile time (reference hash
 // sampler, no injected negatives, MUFU x^b and approximate division), which
 // removes the per-negative and per-term uniform branches of the general path.
 template <int D, bool DENS, int NR, bool COH, int KU, bool FAST>
-__device__ __forceinline__ void process_batch(const EpochArgs &A, WarpSmem<D, KU> &S, uint32_t q0, uint32_t cnt,
-                                              uint32_t node0, int lane, float (&g)[D], bool &act,
-                                              const float *dstat)
+__device__ __forceinline__ void process_batch(const EpochArgs &A, WarpSmem<D, KU> &S, bool live, uint32_t p,
+                                              uint32_t o, uint32_t j, uint32_t edge_local, uint32_t node0,
+                                              int lane, float (&g)[D], bool &act, const float *dstat)
 {
-    const bool live = (uint32_t)lane < cnt;
-    uint32_t j = 32;  // dead lanes: a node of their own, contributing zero
+    if (!live) j = 32;  // dead lanes: a node of their own, contributing zero
     float c[D];
 #pragma unroll
     for (int d = 0; d < D; d++) c[d] = 0.0f;
     if (live) {
-        const uint32_t p = S.qp[q0 + lane], o = S.qo[q0 + lane];
-        j = local_node(S.beg, p);
         const uint32_t self = node0 + j;
-        const uint32_t edge_local = p - S.beg[j];
         float ys[D], yo[D];
 #pragma unroll
         for (int d = 0; d < D; d++) ys[d] = S.ys[j][d];
@@ -403,12 +400,11 @@ __device__ __forceinline__ void epoch_segment(const EpochArgs &A, WarpSmem<D, KU
         uint2 nx = make_uint2(0, 0);
         if (r0 + lane < r1) nx = __ldcs(A.rec + r0 + lane);
         for (uint64_t q = r0; q < r1; q += 32) {
-            const uint32_t cnt = (uint32_t)min((uint64_t)32, r1 - q);
-            S.qp[lane] = nx.x;
-            S.qo[lane] = nx.y;
+            const bool live = q + lane < r1;
+            const uint32_t j = nx.x >> kRecNodeShift, el = nx.x & kRecOffsetMask, o = nx.y;
+            const uint32_t p = live ? S.beg[j] + el : 0u;  // unused (and not loaded) on the fast path
             if (q + 32 + lane < r1) nx = __ldcs(A.rec + q + 32 + lane);
-            __syncwarp();
-            process_batch<D, DENS, NR, COH, KU, FAST>(A, S, 0, cnt, node0, lane, g, act, dstat);
+            process_batch<D, DENS, NR, COH, KU, FAST>(A, S, live, p, o, j, el, node0, lane, g, act, dstat);
         }
     } else {
     const uint32_t seg_beg = S.beg[0], seg_end = S.beg[32];
@@ -448,8 +444,17 @@ __device__ __forceinline__ void epoch_segment(const EpochArgs &A, WarpSmem<D, KU
         // every full batch, and at the end of the segment the remainder too
         const bool last = !more;
         const uint32_t upto = last ? count : (count & ~31u);
-        for (uint32_t q0 = 0; q0 < upto; q0 += 32)
-            process_batch<D, DENS, NR, COH, KU, FAST>(A, S, q0, min(32u, upto - q0), node0, lane, g, act, dstat);
+        for (uint32_t q0 = 0; q0 < upto; q0 += 32) {
+            const bool live = (uint32_t)lane < min(32u, upto - q0);
+            uint32_t p = 0, o = 0, j = 0, el = 0;
+            if (live) {
+                p = S.qp[q0 + lane];
+                o = S.qo[q0 + lane];
+                j = local_node(S.beg, p);
+                el = p - S.beg[j];
+            }
+            process_batch<D, DENS, NR, COH, KU, FAST>(A, S, live, p, o, j, el, node0, lane, g, act, dstat);
+        }
         const uint32_t rem = count - upto;
         if (upto && rem) {
             uint32_t tp = 0, to = 0;

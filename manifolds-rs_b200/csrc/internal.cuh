@@ -197,9 +197,13 @@ void knn_rank_dev(const float *d_x, uint32_t n, uint32_t dim, const uint32_t *d_
                   const uint32_t *d_nbr, uint32_t k, uint32_t metric, uint32_t *d_counts, cudaStream_t s);
 
 // Per-epoch lists of active CSR entries (schedule.cu): rec [n_records]
-// (CSR position, other endpoint); ptr [n_epochs * n_units + 1] record
-// offsets per (epoch, work unit); unit_base [nseg + 1] each segment's first
-// work unit.
+// (entry, other endpoint), the entry packed as (node index within its
+// 32-node segment << kRecNodeShift) | offset within the node's row;
+// ptr [n_epochs * n_units + 1] record offsets per (epoch, work unit);
+// unit_base [nseg + 1] each segment's first work unit. Lists are not built
+// for a graph with a node of kRecOffsetMask + 1 or more entries.
+constexpr uint32_t kRecNodeShift = 27;
+constexpr uint32_t kRecOffsetMask = (1u << kRecNodeShift) - 1u;
 struct ScheduleLists {
     DevBuf<uint2> rec;
     DevBuf<uint64_t> ptr;

@@ -39,11 +39,12 @@ namespace umapcu {
 template <int D, bool DENS, int NR, bool FAST = false, bool LIST = false>
 __global__ void __launch_bounds__(kWarps * 32, 6) k_epoch(const EpochArgs A)
 {
-    __shared__ WarpSmem<D> smem[kWarps];
+    constexpr int KU = LIST ? 1 : kU;  // the list path keeps no scan queue
+    __shared__ WarpSmem<D, KU> smem[kWarps];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t node0 = (blockIdx.x * kWarps + warp) * 32u;
     if (node0 >= A.n) return;
-    epoch_segment<D, DENS, NR, false, kU, FAST, LIST>(A, smem[warp], node0, lane);
+    epoch_segment<D, DENS, NR, false, KU, FAST, LIST>(A, smem[warp], node0, lane);
 }
 
 // ------------------------------------------------------------ densMAP

@@ -10,7 +10,9 @@
 // kernel then reads only those records instead of streaming every entry's
 // (cursor, period) and other endpoint each epoch.
 //
-// Layout: rec [R] = (CSR position, other endpoint) of the active entries,
+// Layout: rec [R] = (packed entry, other endpoint) of the active entries
+// (the entry as its node's index in the segment and its offset in the node's
+// row, so the epoch kernel needs no search for the node),
 // epoch-major, then work unit (units of a segment adjacent), then CSR order;
 // ptr [n_epochs * n_units + 1] = exclusive scan of the per-(epoch, unit)
 // counts and unit_base [nseg + 1] the segments' first units, so epoch e,
@@ -42,10 +44,26 @@ __global__ void k_sched_units(const uint32_t *__restrict__ offsets, uint32_t n, 
     units[s] = len ? (len + kSchedCap - 1) / kSchedCap : 1u;
 }
 
+// packed[p] = (node & 31) << kRecNodeShift | (p - offsets[node]) for every
+// CSR entry p of node; *too_long set when a row does not fit the offset field
+__global__ void k_sched_pack(const uint32_t *__restrict__ offsets, uint32_t n, uint32_t *__restrict__ packed,
+                             uint32_t *__restrict__ too_long)
+{
+    const uint32_t node = blockIdx.x * blockDim.x + threadIdx.x;
+    if (node >= n) return;
+    const uint32_t b = offsets[node], e = offsets[node + 1];
+    if (e - b > kRecOffsetMask + 1u) {
+        *too_long = 1u;
+        return;
+    }
+    for (uint32_t p = b; p < e; p++) packed[p] = ((node & 31u) << kRecNodeShift) | (p - b);
+}
+
 // One warp per unit. counts [n_epochs][n_units] (pass 1) or, with rec
 // non-null, the records written from ptr (pass 2).
 __global__ void __launch_bounds__(kSchedWarps * 32) k_sched_lists(const uint32_t *__restrict__ offsets,
                                                                   const uint32_t *__restrict__ other,
+                                                                  const uint32_t *__restrict__ packed,
                                                                   const float2 *__restrict__ sched, uint32_t n,
                                                                   uint32_t nseg, const uint32_t *__restrict__ unit_base,
                                                                   uint32_t n_units, uint32_t n_epochs,
@@ -90,7 +108,7 @@ __global__ void __launch_bounds__(kSchedWarps * 32) k_sched_lists(const uint32_t
                 if (a) my[i].x = c.x + c.y;
             }
             const unsigned m = __ballot_sync(0xFFFFFFFFu, a);
-            if (rec && a) rec[pos + __popc(m & lt)] = make_uint2(beg + i, other[beg + i]);
+            if (rec && a) rec[pos + __popc(m & lt)] = make_uint2(packed[beg + i], other[beg + i]);
             pos += __popc(m);
             cnt += __popc(m);
         }
@@ -138,9 +156,15 @@ bool build_schedule_lists(const DeviceCsr &csr, uint32_t n_epochs, ScheduleLists
         check_cuda(cub::DeviceScan::InclusiveSum(tmp.p, tb, units.p, unit_base.p + 1, (int64_t)nseg, s), "scan");
     }
     check_cuda(cudaMemsetAsync(unit_base.p, 0, sizeof(uint32_t), s), "memset");
-    uint32_t n_units = 0;
+    DevBuf<uint32_t> packed(2 * csr.n_edges, s), too_long(1, s);
+    check_cuda(cudaMemsetAsync(too_long.p, 0, sizeof(uint32_t), s), "memset");
+    k_sched_pack<<<ceil_div(n, 256), 256, 0, s>>>(csr.offsets.p, n, packed.p, too_long.p);
+    check_launch("k_sched_pack");
+    uint32_t n_units = 0, long_row = 0;
     d2h(&n_units, unit_base.p + nseg, 1, s);
+    d2h(&long_row, too_long.p, 1, s);
     sync(s);
+    if (long_row) return false;
     const uint64_t cells = (uint64_t)n_epochs * n_units;
     const size_t smem = (size_t)kSchedWarps * kSchedCap * sizeof(float2);
     const unsigned grid = ceil_div(n_units, kSchedWarps);
@@ -148,8 +172,8 @@ bool build_schedule_lists(const DeviceCsr &csr, uint32_t n_epochs, ScheduleLists
                "smem attribute");
     DevBuf<uint32_t> counts(cells, s);
     lap("units");
-    k_sched_lists<<<grid, kSchedWarps * 32, smem, s>>>(csr.offsets.p, csr.other.p, csr.sched.p, n, nseg, unit_base.p,
-                                                       n_units, n_epochs, counts.p, nullptr, nullptr);
+    k_sched_lists<<<grid, kSchedWarps * 32, smem, s>>>(csr.offsets.p, csr.other.p, packed.p, csr.sched.p, n, nseg,
+                                                       unit_base.p, n_units, n_epochs, counts.p, nullptr, nullptr);
     check_launch("k_sched_lists count");
     lap("count");
     DevBuf<uint64_t> ptr(cells + 1, s);
@@ -176,8 +200,8 @@ bool build_schedule_lists(const DeviceCsr &csr, uint32_t n_epochs, ScheduleLists
     }
     DevBuf<uint2> rec(R ? R : 1, s);
     lap("alloc rec");
-    k_sched_lists<<<grid, kSchedWarps * 32, smem, s>>>(csr.offsets.p, csr.other.p, csr.sched.p, n, nseg, unit_base.p,
-                                                       n_units, n_epochs, nullptr, ptr.p, rec.p);
+    k_sched_lists<<<grid, kSchedWarps * 32, smem, s>>>(csr.offsets.p, csr.other.p, packed.p, csr.sched.p, n, nseg,
+                                                       unit_base.p, n_units, n_epochs, nullptr, ptr.p, rec.p);
     check_launch("k_sched_lists fill");
     lap("fill");
     out.rec = std::move(rec);
