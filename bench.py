@@ -39,6 +39,15 @@ for _p in (ROOT, os.path.join(ROOT, "manifolds-rs_b200")):
 METRIC = "UMAP layout edge-updates/s (1M pts)"
 UNIT = "edge-updates/s"
 
+
+def metric_of(wl):
+    """The headline metric's name for the 1M-point layout; the other layout
+    workloads name their own size."""
+    if wl["n"] == 1_000_000 and not wl["dens"]:
+        return METRIC
+    size = f"{wl['n'] // 1000}k pts" if wl["n"] < 1_000_000 else f"{wl['n'] / 1e6:g}M pts"
+    return f"UMAP layout edge-updates/s ({size}{', densMAP' if wl['dens'] else ''})"
+
 WORKLOADS = {
     "c2": dict(n=1_000_000, dim=50, clusters=30, k=15, n_epochs=200, kind="anisotropic", dens=False,
                desc="1M x 50 f32, 30-component anisotropic Gaussian mixture (eig log-U[0.1,4], Dirichlet(1) "
@@ -442,7 +451,7 @@ def main():
         dens_launches = 4 * sum(1 for e in range(n_ep) if dp.is_active(e, n_ep))
     if rank == 0:
         out = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "metric": metric_of(wl), "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"{args.workload}: {wl['desc']}", "n_points": wl["n"], "n_edges": int(E),
@@ -705,7 +714,7 @@ def run_reference(args, wl, world):
         samples.append(s)
         secs += t
     value = updates / secs
-    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+    out = {"metric": metric_of(wl), "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": round(secs / args.steps * 1e3, 3), "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
            "config": {"workload": f"{args.workload}: {wl['desc']}", "n_points": wl["n"]},
