@@ -222,10 +222,13 @@ __device__ __forceinline__ uint32_t local_node(const uint32_t *beg, uint32_t p)
 // FAST: the common configuration resolved at compile time (reference hash
 // sampler, no injected negatives, MUFU x^b and approximate division), which
 // removes the per-negative and per-term uniform branches of the general path.
-template <int D, bool DENS, int NR, bool COH, int KU, bool FAST>
-__device__ __forceinline__ void process_batch(const EpochArgs &A, WarpSmem<D, KU> &S, bool live, uint32_t p,
-                                              uint32_t o, uint32_t j, uint32_t edge_local, uint32_t node0,
-                                              int lane, float (&g)[D], bool &act, const float *dstat)
+// The batch's per-node sums go to part[j] for the nodes in the returned
+// mask; unless SPLIT, the node's lane then adds them to g (and sets act).
+template <int D, bool DENS, int NR, bool COH, int KU, bool FAST, bool SPLIT = false>
+__device__ __forceinline__ unsigned process_batch(const EpochArgs &A, WarpSmem<D, KU> &S, bool live, uint32_t p,
+                                                  uint32_t o, uint32_t j, uint32_t edge_local, uint32_t node0,
+                                                  int lane, float (&g)[D], bool &act, const float *dstat,
+                                                  float (*part)[D])
 {
     if (!live) j = 32;  // dead lanes: a node of their own, contributing zero
     float c[D];
@@ -349,16 +352,70 @@ __device__ __forceinline__ void process_batch(const EpochArgs &A, WarpSmem<D, KU
     const bool tail = live && (lane == 31 || jnext != j);
     if (tail) {
 #pragma unroll
-        for (int d = 0; d < D; d++) S.part[j][d] = c[d];
+        for (int d = 0; d < D; d++) part[j][d] = c[d];
     }
     const unsigned has = __reduce_or_sync(kFull, tail ? (1u << j) : 0u);
-    __syncwarp();
-    if ((has >> lane) & 1u) {
-        act = true;
+    if constexpr (!SPLIT) {
+        __syncwarp();
+        if ((has >> lane) & 1u) {
+            act = true;
 #pragma unroll
-        for (int d = 0; d < D; d++) g[d] += S.part[lane][d];
+            for (int d = 0; d < D; d++) g[d] += part[lane][d];
+        }
+        __syncwarp();
     }
-    __syncwarp();
+    return has;
+}
+
+// The segment's row starts, positions (and densMAP node data) into shared
+// memory; ys = the lane's node's position (zeros beyond n).
+template <int D, bool DENS, bool COH, int KU>
+__device__ __forceinline__ void load_segment(const EpochArgs &A, WarpSmem<D, KU> &S, uint32_t node0, int lane,
+                                             float (&ys)[D])
+{
+    const uint32_t node = node0 + lane;
+    const bool valid = node < A.n;
+    S.beg[lane] = A.offsets[valid ? node : A.n];
+    if (lane == 31) S.beg[32] = A.offsets[min(node0 + 32u, A.n)];
+    if (valid) load_row<D, COH>(A.y_cur, node, ys);
+    else {
+#pragma unroll
+        for (int d = 0; d < D; d++) ys[d] = 0.0f;
+    }
+#pragma unroll
+    for (int d = 0; d < D; d++) S.ys[lane][d] = ys[d];
+    if constexpr (DENS) {
+        if (valid) S.dn[lane] = __ldg(A.dens_node + node);
+    }
+}
+
+// The node's step (umap_adam_update, umap_optimiser_gpu.rs:887-923, or the
+// SGD step) from its gradient g, and the next embedding buffer's row.
+template <int D, bool COH>
+__device__ __forceinline__ void finish_node(const EpochArgs &A, uint32_t node, const float (&ys)[D],
+                                            const float (&g)[D], bool act)
+{
+    float yn[D];
+    if (act) {
+        if (A.optimiser == UMAPCU_OPT_SGD) {
+#pragma unroll
+            for (int d = 0; d < D; d++) yn[d] = ys[d] + A.lr_sgd * g[d];
+        } else {
+            float m[D], v[D];
+            load_row<D, COH>(A.m, node, m);
+            load_row<D, COH>(A.v, node, v);
+#pragma unroll
+            for (int d = 0; d < D; d++) yn[d] = adam_coord(g[d], m[d], v[d], ys[d], A.fused, A.epsc, A.omb1, A.omb2);
+            store_row<D>(A.m, node, m);
+            store_row<D>(A.v, node, v);
+        }
+    } else {
+#pragma unroll
+        for (int d = 0; d < D; d++) yn[d] = ys[d];
+    }
+    store_row<D>(A.y_next, node, yn);
+    if (A.dbg_grad) store_row<D>(A.dbg_grad, node, g);
+    if (A.dbg_active) A.dbg_active[node] = act ? 1u : 0u;
 }
 
 // One epoch of one 32-node segment [node0, node0 + 32) of problem A, run by
@@ -371,20 +428,9 @@ __device__ __forceinline__ void epoch_segment(const EpochArgs &A, WarpSmem<D, KU
     __syncwarp();  // the warp's shared memory may still be read by its previous segment
     const uint32_t node = node0 + lane;
     const bool valid = node < A.n;
-    S.beg[lane] = A.offsets[valid ? node : A.n];
-    if (lane == 31) S.beg[32] = A.offsets[min(node0 + 32u, A.n)];
     float ys[D];
-    if (valid) load_row<D, COH>(A.y_cur, node, ys);
-    else {
-#pragma unroll
-        for (int d = 0; d < D; d++) ys[d] = 0.0f;
-    }
-#pragma unroll
-    for (int d = 0; d < D; d++) S.ys[lane][d] = ys[d];
+    load_segment<D, DENS, COH>(A, S, node0, lane, ys);
     const float *dstat = A.dens_stats;
-    if constexpr (DENS) {
-        if (valid) S.dn[lane] = __ldg(A.dens_node + node);
-    }
     // Degenerate self beyond the last beg (beg[32] read by the search only
     // through j + step <= 31 + 1).
     float g[D];
@@ -404,7 +450,7 @@ __device__ __forceinline__ void epoch_segment(const EpochArgs &A, WarpSmem<D, KU
             const uint32_t j = nx.x >> kRecNodeShift, el = nx.x & kRecOffsetMask, o = nx.y;
             const uint32_t p = live ? S.beg[j] + el : 0u;  // unused (and not loaded) on the fast path
             if (q + 32 + lane < r1) nx = __ldcs(A.rec + q + 32 + lane);
-            process_batch<D, DENS, NR, COH, KU, FAST>(A, S, live, p, o, j, el, node0, lane, g, act, dstat);
+            process_batch<D, DENS, NR, COH, KU, FAST>(A, S, live, p, o, j, el, node0, lane, g, act, dstat, S.part);
         }
     } else {
     const uint32_t seg_beg = S.beg[0], seg_end = S.beg[32];
@@ -453,7 +499,7 @@ __device__ __forceinline__ void epoch_segment(const EpochArgs &A, WarpSmem<D, KU
                 j = local_node(S.beg, p);
                 el = p - S.beg[j];
             }
-            process_batch<D, DENS, NR, COH, KU, FAST>(A, S, live, p, o, j, el, node0, lane, g, act, dstat);
+            process_batch<D, DENS, NR, COH, KU, FAST>(A, S, live, p, o, j, el, node0, lane, g, act, dstat, S.part);
         }
         const uint32_t rem = count - upto;
         if (upto && rem) {
@@ -467,27 +513,64 @@ __device__ __forceinline__ void epoch_segment(const EpochArgs &A, WarpSmem<D, KU
     }
     }
     if (!valid) return;
-    float yn[D];
-    if (act) {
-        if (A.optimiser == UMAPCU_OPT_SGD) {
+    finish_node<D, COH>(A, node, ys, g, act);
+}
+
+// One epoch of one 32-node segment run by all kWarps warps of a block, for
+// problems too small to fill the GPU with one warp per segment (schedule
+// lists only). The segment's batches are the same 32-record slices of its
+// list as in epoch_segment; in each round warp w evaluates batch
+// round * kWarps + w into its own part[w], and warp 0's node lanes add the
+// round's partials in batch order -- the order epoch_segment adds them in, so
+// the result is bit-identical.
+template <int D, bool DENS, int NR, bool FAST>
+__device__ __forceinline__ void epoch_segment_split(const EpochArgs &A, WarpSmem<D, 1> &S, float (*part)[32][D],
+                                                    unsigned *has_w, uint32_t node0, int warp, int lane)
+{
+    const uint32_t node = node0 + lane;
+    const bool valid = node < A.n;
+    float ys[D];
+    if (warp == 0) load_segment<D, DENS, false>(A, S, node0, lane, ys);
+    __syncthreads();
+    const float *dstat = A.dens_stats;
+    float g[D];
 #pragma unroll
-            for (int d = 0; d < D; d++) yn[d] = ys[d] + A.lr_sgd * g[d];
-        } else {
-            float m[D], v[D];
-            load_row<D, COH>(A.m, node, m);
-            load_row<D, COH>(A.v, node, v);
-#pragma unroll
-            for (int d = 0; d < D; d++) yn[d] = adam_coord(g[d], m[d], v[d], ys[d], A.fused, A.epsc, A.omb1, A.omb2);
-            store_row<D>(A.m, node, m);
-            store_row<D>(A.v, node, v);
+    for (int d = 0; d < D; d++) g[d] = 0.0f;
+    bool act = false;
+    const uint32_t sg = node0 >> 5;
+    const uint64_t r0 = A.seg_ptr[A.seg_unit[sg]], r1 = A.seg_ptr[A.seg_unit[sg + 1]];
+    const uint64_t stride = 32u * kWarps;
+    uint2 nx = make_uint2(0, 0);
+    if (r0 + 32u * warp + lane < r1) nx = __ldcs(A.rec + r0 + 32u * warp + lane);
+    for (uint64_t q0 = r0; q0 < r1; q0 += stride) {  // block-uniform
+        const uint64_t q = q0 + 32u * warp;
+        unsigned has = 0;
+        if (q < r1) {  // warp-uniform
+            const bool live = q + lane < r1;
+            const uint32_t j = nx.x >> kRecNodeShift, el = nx.x & kRecOffsetMask, o = nx.y;
+            const uint32_t p = live ? S.beg[j] + el : 0u;
+            if (q + stride + lane < r1) nx = __ldcs(A.rec + q + stride + lane);
+            float gd[D];
+            bool ad = false;
+            has = process_batch<D, DENS, NR, false, 1, FAST, true>(A, S, live, p, o, j, el, node0, lane, gd, ad,
+                                                                   dstat, part[warp]);
         }
-    } else {
+        if (lane == 0) has_w[warp] = has;
+        __syncthreads();
+        if (warp == 0) {
 #pragma unroll
-        for (int d = 0; d < D; d++) yn[d] = ys[d];
+            for (int w = 0; w < kWarps; w++) {
+                if ((has_w[w] >> lane) & 1u) {
+                    act = true;
+#pragma unroll
+                    for (int d = 0; d < D; d++) g[d] += part[w][lane][d];
+                }
+            }
+        }
+        __syncthreads();
     }
-    store_row<D>(A.y_next, node, yn);
-    if (A.dbg_grad) store_row<D>(A.dbg_grad, node, g);
-    if (A.dbg_active) A.dbg_active[node] = act ? 1u : 0u;
+    if (warp != 0 || !valid) return;
+    finish_node<D, false>(A, node, ys, g, act);
 }
 
 }  // namespace umapcu

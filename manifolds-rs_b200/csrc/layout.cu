@@ -47,6 +47,18 @@ __global__ void __launch_bounds__(kWarps * 32, 6) k_epoch(const EpochArgs A)
     epoch_segment<D, DENS, NR, false, KU, FAST, LIST>(A, smem[warp], node0, lane);
 }
 
+// Schedule lists on a problem too small to fill the GPU with one warp per
+// segment: one block (kWarps warps) per segment, see epoch_segment_split.
+template <int D, bool DENS, int NR, bool FAST>
+__global__ void __launch_bounds__(kWarps * 32) k_epoch_split(const EpochArgs A)
+{
+    __shared__ WarpSmem<D, 1> seg;
+    __shared__ float part[kWarps][32][D];
+    __shared__ unsigned has_w[kWarps];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    epoch_segment_split<D, DENS, NR, FAST>(A, seg, part, has_w, blockIdx.x * 32u, warp, lane);
+}
+
 // ------------------------------------------------------------ densMAP
 
 constexpr int kDensBlock = 256;
@@ -248,13 +260,21 @@ static void set_carveout()
     }
 }
 
+// Below this many segments (about 9 blocks of one warp per segment on each
+// of the 148 SMs) the list path gives each segment a whole block.
+constexpr uint32_t kSplitSegments = 148 * 9;
+
 template <int D, bool DENS>
 static void launch_epoch_t(const EpochArgs &A, cudaStream_t s)
 {
     const uint32_t nseg = ceil_div(A.n, 32);
     const bool fast = !A.injected && A.sampler == UMAPCU_NEG_REF_HASH && !A.precise_pow;
     const unsigned grid = ceil_div(nseg, kWarps);
-    if (A.rec) {
+    if (A.rec && nseg < kSplitSegments) {
+        if (A.neg_rate == 5 && fast) k_epoch_split<D, DENS, 5, true><<<nseg, kWarps * 32, 0, s>>>(A);
+        else if (A.neg_rate == 5) k_epoch_split<D, DENS, 5, false><<<nseg, kWarps * 32, 0, s>>>(A);
+        else k_epoch_split<D, DENS, 0, false><<<nseg, kWarps * 32, 0, s>>>(A);
+    } else if (A.rec) {
         if (A.neg_rate == 5 && fast) k_epoch<D, DENS, 5, true, true><<<grid, kWarps * 32, 0, s>>>(A);
         else if (A.neg_rate == 5) k_epoch<D, DENS, 5, false, true><<<grid, kWarps * 32, 0, s>>>(A);
         else k_epoch<D, DENS, 0, false, true><<<grid, kWarps * 32, 0, s>>>(A);

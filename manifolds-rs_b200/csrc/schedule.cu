@@ -30,10 +30,12 @@ namespace {
 
 constexpr int kSchedWarps = 4;
 // A work unit is at most kSchedCap consecutive CSR entries of one segment
-// (a segment of L entries has ceil(L / kSchedCap) units, at least one): one
-// warp per unit keeps the unit's cursors in shared memory and walks epoch by
-// epoch, so a hub-heavy segment does not hold one warp for its whole length.
-constexpr uint32_t kSchedCap = 1024;
+// (a segment of L entries has ceil(L / kSchedCap) units, at least one). One
+// warp per unit: lane l owns the unit's entries l, l + 32, ..., and keeps
+// their (cursor, period) -- and, when filling, their record fields -- in
+// registers for the whole walk over the epochs.
+constexpr uint32_t kSchedPer = 8;
+constexpr uint32_t kSchedCap = 32 * kSchedPer;
 
 __global__ void k_sched_units(const uint32_t *__restrict__ offsets, uint32_t n, uint32_t nseg,
                               uint32_t *__restrict__ units)
@@ -42,6 +44,14 @@ __global__ void k_sched_units(const uint32_t *__restrict__ offsets, uint32_t n, 
     if (s >= nseg) return;
     const uint32_t len = offsets[min(s * 32u + 32u, n)] - offsets[s * 32u];
     units[s] = len ? (len + kSchedCap - 1) / kSchedCap : 1u;
+}
+
+// unit_seg[u] = the segment of work unit u
+__global__ void k_sched_unit_seg(const uint32_t *__restrict__ unit_base, uint32_t nseg, uint32_t *__restrict__ unit_seg)
+{
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nseg) return;
+    for (uint32_t u = unit_base[s]; u < unit_base[s + 1]; u++) unit_seg[u] = s;
 }
 
 // packed[p] = (node & 31) << kRecNodeShift | (p - offsets[node]) for every
@@ -59,60 +69,67 @@ __global__ void k_sched_pack(const uint32_t *__restrict__ offsets, uint32_t n, u
     for (uint32_t p = b; p < e; p++) packed[p] = ((node & 31u) << kRecNodeShift) | (p - b);
 }
 
-// One warp per unit. counts [n_epochs][n_units] (pass 1) or, with rec
-// non-null, the records written from ptr (pass 2).
+// One warp per unit. FILL = false: counts [n_epochs][n_units]; FILL = true:
+// the records, written from ptr.
+template <bool FILL>
 __global__ void __launch_bounds__(kSchedWarps * 32) k_sched_lists(const uint32_t *__restrict__ offsets,
                                                                   const uint32_t *__restrict__ other,
                                                                   const uint32_t *__restrict__ packed,
                                                                   const float2 *__restrict__ sched, uint32_t n,
-                                                                  uint32_t nseg, const uint32_t *__restrict__ unit_base,
+                                                                  const uint32_t *__restrict__ unit_seg,
+                                                                  const uint32_t *__restrict__ unit_base,
                                                                   uint32_t n_units, uint32_t n_epochs,
                                                                   uint32_t *__restrict__ counts,
                                                                   const uint64_t *__restrict__ ptr,
                                                                   uint2 *__restrict__ rec)
 {
-    extern __shared__ float2 cur[];  // [kSchedWarps][kSchedCap] (cursor, period)
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t u = blockIdx.x * kSchedWarps + warp;
     if (u >= n_units) return;  // warp-uniform
-    // the unit's segment: largest s with unit_base[s] <= u
-    uint32_t lo = 0, hi = nseg;
-    while (hi - lo > 1) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (unit_base[mid] <= u) lo = mid;
-        else hi = mid;
-    }
-    const uint32_t s = lo, piece = u - unit_base[s];
-    const uint32_t sbeg = offsets[s * 32u], send = offsets[min(s * 32u + 32u, n)];
+    const uint32_t sg = unit_seg[u], piece = u - unit_base[sg];
+    const uint32_t sbeg = offsets[sg * 32u], send = offsets[min(sg * 32u + 32u, n)];
     const uint32_t beg = min(send, sbeg + piece * kSchedCap), end = min(send, beg + kSchedCap);
-    const uint32_t len = end - beg;
-    float2 *my = cur + (size_t)warp * kSchedCap;
     const unsigned lt = (1u << lane) - 1u;
-    for (uint32_t i = lane; i < len; i += 32) {
-        const float per = sched[beg + i].y;
-        my[i] = make_float2(per, per);  // reset state: cursor = period
+    float cur[kSchedPer], per[kSchedPer];
+    uint2 rv[kSchedPer];
+#pragma unroll
+    for (uint32_t t = 0; t < kSchedPer; t++) {
+        const uint32_t p = beg + 32u * t + lane;
+        cur[t] = __int_as_float(0x7f800000);  // beyond the unit: never active
+        per[t] = 0.0f;
+        rv[t] = make_uint2(0, 0);
+        if (p < end) {
+            per[t] = sched[p].y;
+            cur[t] = per[t];  // reset state: cursor = period
+            if (FILL) rv[t] = make_uint2(packed[p], other[p]);
+        }
     }
-    __syncwarp();
-    uint64_t bases = 0;  // lane l: the cell offset of epoch (e & ~31) + l
+    uint64_t bases = 0;  // lane l: the record offset of epoch (e & ~31) + l
+    uint32_t mine = 0;   // lane l: the count of epoch (e & ~31) + l
     for (uint32_t e = 0; e < n_epochs; e++) {
         const float ef = (float)e;
-        if (rec && (e & 31) == 0 && e + lane < n_epochs) bases = ptr[(size_t)(e + lane) * n_units + u];
-        uint64_t pos = rec ? __shfl_sync(0xFFFFFFFFu, bases, e & 31) : 0;
+        if (FILL && (e & 31) == 0 && e + lane < n_epochs) bases = ptr[(size_t)(e + lane) * n_units + u];
+        uint64_t pos = FILL ? __shfl_sync(0xFFFFFFFFu, bases, e & 31) : 0;
         uint32_t cnt = 0;
-        for (uint32_t i0 = 0; i0 < len; i0 += 32) {
-            const uint32_t i = i0 + lane;
-            bool a = false;
-            if (i < len) {
-                const float2 c = my[i];
-                a = c.x <= ef;
-                if (a) my[i].x = c.x + c.y;
-            }
+#pragma unroll
+        for (uint32_t t = 0; t < kSchedPer; t++) {
+            const bool a = cur[t] <= ef;
+            if (a) cur[t] = cur[t] + per[t];
             const unsigned m = __ballot_sync(0xFFFFFFFFu, a);
-            if (rec && a) rec[pos + __popc(m & lt)] = make_uint2(packed[beg + i], other[beg + i]);
-            pos += __popc(m);
-            cnt += __popc(m);
+            if (FILL) {
+                if (a) rec[pos + __popc(m & lt)] = rv[t];
+                pos += __popc(m);
+            } else {
+                cnt += __popc(m);
+            }
         }
-        if (!rec && lane == 0) counts[(size_t)e * n_units + u] = cnt;
+        if (!FILL) {
+            if (lane == (e & 31)) mine = cnt;
+            if ((e & 31) == 31 || e + 1 == n_epochs) {
+                const uint32_t e0 = e & ~31u;
+                if (e0 + lane <= e) counts[(size_t)(e0 + lane) * n_units + u] = mine;
+            }
+        }
     }
 }
 
@@ -165,15 +182,16 @@ bool build_schedule_lists(const DeviceCsr &csr, uint32_t n_epochs, ScheduleLists
     d2h(&long_row, too_long.p, 1, s);
     sync(s);
     if (long_row) return false;
+    DevBuf<uint32_t> unit_seg(n_units, s);
+    k_sched_unit_seg<<<ceil_div(nseg, 256), 256, 0, s>>>(unit_base.p, nseg, unit_seg.p);
+    check_launch("k_sched_unit_seg");
     const uint64_t cells = (uint64_t)n_epochs * n_units;
-    const size_t smem = (size_t)kSchedWarps * kSchedCap * sizeof(float2);
     const unsigned grid = ceil_div(n_units, kSchedWarps);
-    check_cuda(cudaFuncSetAttribute(k_sched_lists, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-               "smem attribute");
     DevBuf<uint32_t> counts(cells, s);
     lap("units");
-    k_sched_lists<<<grid, kSchedWarps * 32, smem, s>>>(csr.offsets.p, csr.other.p, packed.p, csr.sched.p, n, nseg,
-                                                       unit_base.p, n_units, n_epochs, counts.p, nullptr, nullptr);
+    k_sched_lists<false><<<grid, kSchedWarps * 32, 0, s>>>(csr.offsets.p, csr.other.p, packed.p, csr.sched.p, n,
+                                                          unit_seg.p, unit_base.p, n_units, n_epochs, counts.p,
+                                                          nullptr, nullptr);
     check_launch("k_sched_lists count");
     lap("count");
     DevBuf<uint64_t> ptr(cells + 1, s);
@@ -200,8 +218,9 @@ bool build_schedule_lists(const DeviceCsr &csr, uint32_t n_epochs, ScheduleLists
     }
     DevBuf<uint2> rec(R ? R : 1, s);
     lap("alloc rec");
-    k_sched_lists<<<grid, kSchedWarps * 32, smem, s>>>(csr.offsets.p, csr.other.p, packed.p, csr.sched.p, n, nseg,
-                                                       unit_base.p, n_units, n_epochs, nullptr, ptr.p, rec.p);
+    k_sched_lists<true><<<grid, kSchedWarps * 32, 0, s>>>(csr.offsets.p, csr.other.p, packed.p, csr.sched.p, n,
+                                                         unit_seg.p, unit_base.p, n_units, n_epochs, nullptr, ptr.p,
+                                                         rec.p);
     check_launch("k_sched_lists fill");
     lap("fill");
     out.rec = std::move(rec);

@@ -2,7 +2,9 @@
 the per-epoch CSR scan: the same active entries in the same CSR order and
 batch boundaries, so results must agree bit for bit, for in-order runs, for
 runs that skip epochs (the state falls back to the scan), after reset, and
-with the densMAP term (needs a B200)."""
+with the densMAP term (needs a B200). The small problems run the list path
+with a block per segment; the 60k-point one runs it with a warp per
+segment."""
 import os
 
 import numpy as np
@@ -79,3 +81,25 @@ def test_lists_equal_scan_densmap():
     a.run(0, 60)
     b.run(0, 60)
     assert np.array_equal(a.read()[0], b.read()[0])
+
+
+def test_lists_equal_scan_warp_per_segment():
+    import umapcu.synth as S
+    n = 60000  # 1875 segments: above the block-per-segment threshold
+    X, _ = S.isotropic_mixture(n, 20, 10, 3)
+    idx, dist = umapcu.knn_exact(X, 15)
+    graph = umapcu.construct_umap_graph(idx, dist, umapcu.UmapGraphParams(), 40)
+    adj = umapcu.coo_to_adjacency_list(graph)
+    p = umapcu.UmapOptimParams(n_epochs=40)
+    emb = init_embedding(n, 2, seed=5)
+    a, b = _state(adj, emb, p, True), _state(adj, emb, p, False)
+    assert a.schedule_info()["lists"] and not b.schedule_info()["lists"]
+    for first, count in [(0, 25), (25, 15)]:
+        a.run(first, count)
+        b.run(first, count)
+        ya, ma, va, ca = a.read()
+        yb, mb, vb, cb = b.read()
+        assert np.array_equal(ya, yb) and np.array_equal(ma, mb) and np.array_equal(va, vb)
+        assert np.array_equal(ca, cb)
+    a.close()
+    b.close()
