@@ -463,6 +463,8 @@ def main():
                        "schedule": ("per-epoch active-entry lists built at state creation "
                                     f"({sched['build_ms']:.1f} ms, {sched['records']} records; outside the timed "
                                     "region like the CSR build)") if sched["lists"] else "CSR scan every epoch",
+                       "e2e_schedule": "per-epoch active-entry bitmasks (1 bit per CSR entry and epoch), built "
+                                       "inside each timed call",
                        "value_csr_scan": scan_value,
                        "l2": "flushed before every step (256 MiB write)",
                        "parallelism": f"replicas x{world}"},

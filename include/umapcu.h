@@ -357,9 +357,13 @@ umapcu_status umapcu_sample_negatives(uint32_t sampler, uint64_t seed, uint32_t 
  * (the same f32 cursor arithmetic), so its epochs read those records instead
  * of scanning every entry's cursor. Results are bit-identical to the scan;
  * runs that skip or repeat epochs fall back to the scan until
- * umapcu_state_reset. Set UMAPCU_NO_SCHEDULE_LISTS to disable; the one-shot
- * umapcu_optimise_embedding always scans. lists_active: 1 when built;
- * n_records: records held (8 bytes each); build_ms: build time. */
+ * umapcu_state_reset. The one-shot umapcu_optimise_embedding (and a state
+ * whose lists do not fit in half the free device memory) precomputes the
+ * same schedule as per-epoch bitmasks instead (1 bit per CSR entry and
+ * epoch; its epochs scan the bits in place of the cursors), again
+ * bit-identical. Set UMAPCU_NO_SCHEDULE_LISTS to disable both forms.
+ * lists_active: 1 when lists are built; n_records: records held (8 bytes
+ * each); build_ms: list build time. */
 umapcu_status umapcu_state_schedule_info(const umapcu_state *st, int *lists_active, uint64_t *n_records,
                                          float *build_ms);
 

@@ -45,7 +45,8 @@ struct umapcu_state {
     // 0, 1, ..., sched_epoch - 1 from the reset schedule; the cursors in
     // csr.sched then lag (sched_lazy) until something needs them
     ScheduleLists lists;
-    bool lists_ok = false, sched_continuous = true, sched_lazy = false;
+    ScheduleBits bits;  // the bitmask form, used when there are no lists
+    bool lists_ok = false, bits_ok = false, sched_continuous = true, sched_lazy = false;
     uint32_t sched_epoch = 0;
     float lists_build_ms = 0.0f;
 };
@@ -118,13 +119,17 @@ void run_epoch(umapcu_state *st, uint32_t epoch, uint32_t optimiser, const uint3
     if (dens_on && !skip_dens) dens_update(st);
     const bool in_order = st->sched_continuous && epoch == st->sched_epoch;
     const bool use_lists = st->lists_ok && in_order && epoch < st->lists.n_epochs;
-    if (!use_lists) sync_cursors(st);  // the scan reads and advances the cursors
+    const bool use_bits = !use_lists && st->bits_ok && in_order && epoch < st->bits.n_epochs;
+    if (!use_lists && !use_bits) sync_cursors(st);  // the scan reads and advances the cursors
     if (!in_order) st->sched_continuous = false;
     EpochArgs A{};
     if (use_lists) {
         A.rec = st->lists.rec.p;
         A.seg_ptr = st->lists.ptr.p + (size_t)epoch * st->lists.n_units;
         A.seg_unit = st->lists.unit_base.p;
+        st->sched_lazy = true;
+    } else if (use_bits) {
+        A.bits = st->bits.bits + (size_t)epoch * st->bits.words;
         st->sched_lazy = true;
     }
     if (in_order) st->sched_epoch = epoch + 1;
@@ -214,9 +219,13 @@ umapcu_status create_state(const float *embd, uint32_t n, uint32_t n_dim, const 
         if (rc != UMAPCU_OK) return rc;
         T.mark("CSR build", s);
     }
-    // Schedule lists pay for their build (a few ms at 1M points) over repeated
-    // or resumed runs of a resident state; a one-shot call scans instead.
-    if (lists && !getenv("UMAPCU_NO_SCHEDULE_LISTS")) {
+    // The schedule precomputed for epochs 0 .. n_epochs - 1 (schedule.cu):
+    // record lists pay for their build (~10 ms at 1M points) over repeated or
+    // resumed runs of a resident state; a one-shot call (or a state whose
+    // lists do not fit) takes the bitmasks, built in well under a millisecond.
+    // UMAPCU_NO_SCHEDULE_LISTS set: neither, every epoch scans the cursors.
+    const bool precompute = !getenv("UMAPCU_NO_SCHEDULE_LISTS");
+    if (lists && precompute) {
         sync(s);
         const auto t0 = std::chrono::steady_clock::now();
         st->lists_ok = build_schedule_lists(st->csr, params->n_epochs, st->lists, s);
@@ -224,6 +233,10 @@ umapcu_status create_state(const float *embd, uint32_t n, uint32_t n_dim, const 
         st->lists_build_ms =
             (float)std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         T.mark("schedule lists", s);
+    }
+    if (!st->lists_ok && precompute) {
+        st->bits_ok = build_schedule_bits(st->csr, params->n_epochs, st->bits, s);
+        T.mark("schedule bitmasks", s);
     }
     const uint64_t nt = (uint64_t)n * n_dim;
     st->y[0].alloc(nt, s);

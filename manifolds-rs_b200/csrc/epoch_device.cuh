@@ -422,7 +422,10 @@ __device__ __forceinline__ void finish_node(const EpochArgs &A, uint32_t node, c
 // one warp (see the file comment).
 // LIST: the segment's active entries come from the epoch's schedule lists
 // (A.rec / A.seg_ptr) instead of a scan of its CSR range.
-template <int D, bool DENS, int NR, bool COH, int KU = kU, bool FAST = false, bool LIST = false>
+// BITS: the scan reads the epoch's active-entry bitmask (A.bits) in place of
+// the entries' (cursor, period) and writes no cursor.
+template <int D, bool DENS, int NR, bool COH, int KU = kU, bool FAST = false, bool LIST = false,
+          bool BITS = false>
 __device__ __forceinline__ void epoch_segment(const EpochArgs &A, WarpSmem<D, KU> &S, uint32_t node0, int lane)
 {
     __syncwarp();  // the warp's shared memory may still be read by its previous segment
@@ -461,22 +464,29 @@ __device__ __forceinline__ void epoch_segment(const EpochArgs &A, WarpSmem<D, KU
     // issued before the first is used.
     for (uint32_t c0 = seg_beg; c0 < seg_end; c0 += 32u * KU) {
         float2 sv[KU];
-        uint32_t ov[KU];
+        uint32_t ov[KU], bw[KU];
 #pragma unroll
         for (int u = 0; u < KU; u++) {
             const uint32_t p = c0 + 32u * u + lane;
             sv[u] = make_float2(__int_as_float(0x7f800000), 0.0f);
             ov[u] = 0;
+            bw[u] = 0;
             if (p < seg_end) {
-                sv[u] = COH ? __ldcg(A.sched + p) : __ldcs(A.sched + p);
+                if constexpr (BITS) bw[u] = __ldg(A.bits + (p >> 5));
+                else sv[u] = COH ? __ldcg(A.sched + p) : __ldcs(A.sched + p);
                 ov[u] = __ldcs(A.other + p);
             }
         }
 #pragma unroll
         for (int u = 0; u < KU; u++) {
             const uint32_t p = c0 + 32u * u + lane;
-            const bool a = sv[u].x <= A.epoch_f;  // out-of-range lanes hold +inf
-            if (a) __stcs(cursor + 2 * (uint64_t)p, sv[u].x + sv[u].y);  // umap_edge_schedule_update
+            bool a;
+            if constexpr (BITS) {
+                a = (bw[u] >> (p & 31u)) & 1u;  // out-of-range lanes hold 0
+            } else {
+                a = sv[u].x <= A.epoch_f;  // out-of-range lanes hold +inf
+                if (a) __stcs(cursor + 2 * (uint64_t)p, sv[u].x + sv[u].y);  // umap_edge_schedule_update
+            }
             const unsigned mask = __ballot_sync(kFull, a);
             if (a) {
                 const uint32_t slot = count + __popc(mask & lt_mask);

@@ -215,6 +215,31 @@ struct ScheduleLists {
 // = period); false when they would not fit (half the free device memory) or
 // n_epochs is out of range, `out` then empty.
 bool build_schedule_lists(const DeviceCsr &csr, uint32_t n_epochs, ScheduleLists &out, cudaStream_t s);
+// Per-epoch bitmasks of active CSR entries (schedule.cu): bits
+// [n_epochs][words], bit p & 31 of word p >> 5 of epoch e set when entry p
+// is active in epoch e (words = ceil(2E / 32)). 1 bit per entry and epoch
+// against the lists' 8 bytes per active entry, and built in well under a
+// millisecond at 1M points: the precomputed schedule of a one-shot run.
+// The buffer comes from a per-device cache (one block, grown to the largest
+// request, kept between calls): a one-shot call then allocates no more
+// stream-ordered pool memory than it would without the bitmasks.
+struct ScheduleBits {
+    uint32_t *bits = nullptr;
+    size_t cap = 0;  // words of the held block
+    int dev = -1;
+    cudaStream_t built_on = nullptr;  // synchronised before the block goes back to the cache
+    uint64_t words = 0;
+    uint32_t n_epochs = 0;
+    ScheduleBits() = default;
+    ScheduleBits(const ScheduleBits &) = delete;
+    ScheduleBits &operator=(const ScheduleBits &) = delete;
+    ~ScheduleBits();
+};
+// Builds the bitmasks for epochs [0, n_epochs) from the reset schedule;
+// false when they would not fit (half the free device memory), `out` then
+// empty.
+bool build_schedule_bits(const DeviceCsr &csr, uint32_t n_epochs, ScheduleBits &out, cudaStream_t s);
+
 // Writes into csr.sched the cursors after `epochs` epochs from the reset
 // schedule (the state the per-epoch scan would have left).
 void materialise_schedule(DeviceCsr &csr, uint32_t epochs, cudaStream_t s);

@@ -26,6 +26,12 @@
 // is double-buffered: every gather of an epoch reads the pre-step positions,
 // as the reference's separate gradient and Adam kernels do).
 //
+// With the schedule precomputed (schedule.cu) the kernel either scans the
+// epoch's active-entry bitmask in place of the (cursor, period) pairs (BITS),
+// or reads the epoch's active-entry records without any scan (LIST; a block
+// per segment on small problems, k_epoch_split). All three pick the same
+// entries in the same order, so their results are bit-identical.
+//
 // Arithmetic follows the reference expression by expression with no FMA
 // contraction (compiled with -fmad=false). x^b is evaluated by pow_pos
 // (below) unless the state asks for CUDA's powf; logf/expf are evaluated in
@@ -36,7 +42,7 @@
 
 namespace umapcu {
 
-template <int D, bool DENS, int NR, bool FAST = false, bool LIST = false>
+template <int D, bool DENS, int NR, bool FAST = false, bool LIST = false, bool BITS = false>
 __global__ void __launch_bounds__(kWarps * 32, 6) k_epoch(const EpochArgs A)
 {
     constexpr int KU = LIST ? 1 : kU;  // the list path keeps no scan queue
@@ -44,7 +50,7 @@ __global__ void __launch_bounds__(kWarps * 32, 6) k_epoch(const EpochArgs A)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t node0 = (blockIdx.x * kWarps + warp) * 32u;
     if (node0 >= A.n) return;
-    epoch_segment<D, DENS, NR, false, KU, FAST, LIST>(A, smem[warp], node0, lane);
+    epoch_segment<D, DENS, NR, false, KU, FAST, LIST, BITS>(A, smem[warp], node0, lane);
 }
 
 // Schedule lists on a problem too small to fill the GPU with one warp per
@@ -278,6 +284,10 @@ static void launch_epoch_t(const EpochArgs &A, cudaStream_t s)
         if (A.neg_rate == 5 && fast) k_epoch<D, DENS, 5, true, true><<<grid, kWarps * 32, 0, s>>>(A);
         else if (A.neg_rate == 5) k_epoch<D, DENS, 5, false, true><<<grid, kWarps * 32, 0, s>>>(A);
         else k_epoch<D, DENS, 0, false, true><<<grid, kWarps * 32, 0, s>>>(A);
+    } else if (A.bits) {
+        if (A.neg_rate == 5 && fast) k_epoch<D, DENS, 5, true, false, true><<<grid, kWarps * 32, 0, s>>>(A);
+        else if (A.neg_rate == 5) k_epoch<D, DENS, 5, false, false, true><<<grid, kWarps * 32, 0, s>>>(A);
+        else k_epoch<D, DENS, 0, false, false, true><<<grid, kWarps * 32, 0, s>>>(A);
     } else {
         if (A.neg_rate == 5 && fast) k_epoch<D, DENS, 5, true><<<grid, kWarps * 32, 0, s>>>(A);
         else if (A.neg_rate == 5) k_epoch<D, DENS, 5><<<grid, kWarps * 32, 0, s>>>(A);

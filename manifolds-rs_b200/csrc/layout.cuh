@@ -22,6 +22,7 @@ struct EpochArgs {
     const uint2 *rec;          // schedule lists: (CSR position, other) of active entries, or nullptr (scan)
     const uint64_t *seg_ptr;   // schedule lists: this epoch's record offsets per work unit
     const uint32_t *seg_unit;  // schedule lists: [nseg + 1] each segment's first work unit
+    const uint32_t *bits;      // schedule bitmask of this epoch (bit p: entry p active), or nullptr
     const uint32_t *injected;  // [2E * neg_rate] injected negatives or nullptr
     float *dbg_grad;           // [n * D] gradient output or nullptr
     uint32_t *dbg_active;      // [n] has_update output or nullptr

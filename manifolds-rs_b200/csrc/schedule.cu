@@ -20,6 +20,8 @@
 // ptr[e * n_units + unit_base[s + 1]]).
 #include <chrono>
 #include <cstdlib>
+#include <mutex>
+#include <utility>
 
 #include <cub/cub.cuh>
 
@@ -133,6 +135,33 @@ __global__ void __launch_bounds__(kSchedWarps * 32) k_sched_lists(const uint32_t
     }
 }
 
+// Bitmasks: thread per 32-entry word, the word's cursors and periods in
+// registers, one word written per epoch (coalesced across the warp).
+__global__ void __launch_bounds__(128) k_sched_bits(const float2 *__restrict__ sched, uint64_t n_entries,
+                                                    uint64_t words, uint32_t n_epochs, uint32_t *__restrict__ bits)
+{
+    const uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= words) return;
+    float cur[32], per[32];
+#pragma unroll
+    for (int t = 0; t < 32; t++) {
+        const uint64_t p = w * 32 + t;
+        per[t] = p < n_entries ? sched[p].y : 0.0f;
+        cur[t] = p < n_entries ? per[t] : __int_as_float(0x7f800000);  // reset: cursor = period
+    }
+    for (uint32_t e = 0; e < n_epochs; e++) {
+        const float ef = (float)e;
+        uint32_t word = 0;
+#pragma unroll
+        for (int t = 0; t < 32; t++) {
+            const bool a = cur[t] <= ef;
+            if (a) cur[t] = cur[t] + per[t];
+            word |= (a ? 1u : 0u) << t;
+        }
+        bits[(size_t)e * words + w] = word;
+    }
+}
+
 // Cursors after `epochs` epochs of the schedule from the reset state.
 __global__ void k_sched_materialise(float2 *__restrict__ sched, uint64_t n_entries, uint32_t epochs)
 {
@@ -230,6 +259,71 @@ bool build_schedule_lists(const DeviceCsr &csr, uint32_t n_epochs, ScheduleLists
     out.n_epochs = n_epochs;
     out.nseg = nseg;
     out.n_units = n_units;
+    return true;
+}
+
+namespace {
+
+// One cached bitmask block per device (cudaMalloc, outside the stream-ordered
+// pool); a call that finds it taken by a concurrent call allocates its own.
+std::mutex g_bits_mu;
+struct BitsBlock {
+    uint32_t *p = nullptr;
+    size_t cap = 0;
+};
+BitsBlock g_bits_cache[64];
+
+}  // namespace
+
+ScheduleBits::~ScheduleBits()
+{
+    if (!bits) return;
+    if (built_on) cudaStreamSynchronize(built_on);
+    std::lock_guard<std::mutex> lk(g_bits_mu);
+    if (dev >= 0 && dev < 64 && !g_bits_cache[dev].p) {
+        g_bits_cache[dev] = BitsBlock{bits, cap};
+    } else {
+        cudaFree(bits);  // a concurrent call's block: the cache holds one
+    }
+}
+
+bool build_schedule_bits(const DeviceCsr &csr, uint32_t n_epochs, ScheduleBits &out, cudaStream_t s)
+{
+    const uint64_t entries = 2 * csr.n_edges;
+    if (out.bits || !entries || !n_epochs) return false;
+    const uint64_t words = (entries + 31) / 32;
+    const size_t need = (size_t)n_epochs * words;
+    int dev = 0;
+    check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+    if (dev < 0 || dev >= 64) return false;
+    BitsBlock blk;
+    {
+        std::lock_guard<std::mutex> lk(g_bits_mu);
+        std::swap(blk, g_bits_cache[dev]);
+    }
+    if (blk.cap < need) {
+        if (blk.p) {
+            sync(s);  // the stream may still be using device memory; the block itself is idle
+            cudaFree(blk.p);
+            blk = BitsBlock{};
+        }
+        size_t free_b = 0, total_b = 0;
+        check_cuda(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+        if (need * sizeof(uint32_t) > free_b / 2) return false;
+        if (cudaMalloc((void **)&blk.p, need * sizeof(uint32_t)) != cudaSuccess) {
+            cudaGetLastError();  // an allocation failure is not sticky: no bitmasks, the scan runs
+            return false;
+        }
+        blk.cap = need;
+    }
+    out.bits = blk.p;
+    out.cap = blk.cap;
+    out.dev = dev;
+    out.built_on = s;
+    k_sched_bits<<<ceil_div(words, 128), 128, 0, s>>>(csr.sched.p, entries, words, n_epochs, out.bits);
+    check_launch("k_sched_bits");
+    out.words = words;
+    out.n_epochs = n_epochs;
     return true;
 }
 

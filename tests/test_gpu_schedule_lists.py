@@ -103,3 +103,46 @@ def test_lists_equal_scan_warp_per_segment():
         assert np.array_equal(ca, cb)
     a.close()
     b.close()
+
+
+def _one_shot(adj, emb, p, dens=None, seed=9, precompute=True, opt=None):
+    y = np.ascontiguousarray(emb.copy())
+    old = os.environ.pop("UMAPCU_NO_SCHEDULE_LISTS", None)
+    try:
+        if not precompute:
+            os.environ["UMAPCU_NO_SCHEDULE_LISTS"] = "1"
+        umapcu.optimise_embedding_adam_gpu(y, adj, p, dens, seed, 0, umapcu.NEG_REF_HASH,
+                                           umapcu.OPT_ADAM if opt is None else opt)
+    finally:
+        os.environ.pop("UMAPCU_NO_SCHEDULE_LISTS", None)
+        if old is not None:
+            os.environ["UMAPCU_NO_SCHEDULE_LISTS"] = old
+    return y
+
+
+@pytest.mark.parametrize("opt", ["adam", "sgd"])
+def test_one_shot_bitmask_equals_scan(prob, opt):
+    """The one-shot call runs its epochs on per-epoch bitmasks of the active
+    entries; with the precomputed schedule switched off it scans the
+    cursors, and a scanning state gives the same: all three bit-identical."""
+    g, adj = prob
+    p = umapcu.UmapOptimParams(n_epochs=70)
+    o = umapcu.OPT_SGD if opt == "sgd" else umapcu.OPT_ADAM
+    emb = init_embedding(3000, 2, seed=12)
+    y_bits = _one_shot(adj, emb, p, opt=o)
+    y_scan = _one_shot(adj, emb, p, precompute=False, opt=o)
+    st = _state(adj, emb, p, False)
+    st.run(0, 70, o)
+    assert np.array_equal(y_bits, y_scan)
+    assert np.array_equal(y_bits, st.read()[0])
+    st.close()
+
+
+def test_one_shot_bitmask_equals_scan_densmap_3d():
+    g = oracle_graph(n=2500, dim=30, k=15, n_epochs=60)
+    coo = umapcu.CoordinateList(g["row"], g["col"], g["val"], 2500)
+    dens = umapcu.DensState.new(umapcu.DensParams(), coo, g["idx"], g["dist"], True)
+    adj = umapcu.Adjacency(g["ptr"], g["col"], g["val"])
+    p = umapcu.UmapOptimParams(n_epochs=60)
+    emb = init_embedding(2500, 3, seed=13)
+    assert np.array_equal(_one_shot(adj, emb, p, dens), _one_shot(adj, emb, p, dens, precompute=False))
