@@ -583,4 +583,121 @@ __device__ __forceinline__ void epoch_segment_split(const EpochArgs &A, WarpSmem
     finish_node<D, false>(A, node, ys, g, act);
 }
 
+// Position of the k-th set bit (k from 0) of m, which has more than k set
+// bits: a binary search on popcounts.
+__device__ __forceinline__ uint32_t select_bit(uint32_t m, uint32_t k)
+{
+    uint32_t pos = 0;
+#pragma unroll
+    for (uint32_t w = 16; w > 0; w >>= 1) {
+        const uint32_t c = __popc(m & ((1u << w) - 1u));
+        if (k >= c) {
+            k -= c;
+            m >>= w;
+            pos += w;
+        }
+    }
+    return pos;
+}
+
+// Words of a segment's bitmask one block of epoch_segment_split_bits holds;
+// a longer segment runs on warp 0 alone with the sequential scan.
+constexpr uint32_t kSplitWords = 256;
+
+// The bitmask form of epoch_segment_split: the block reads the segment's
+// words of the epoch's bitmask, masks them to the segment's entries, and
+// forms prefix counts; batch b is then the active entries of rank 32 b ..
+// 32 b + 31 in CSR order -- the batches the sequential scan forms -- and
+// lane t finds its entry by searching the prefix counts and selecting the
+// bit. Partials are added in batch order as in epoch_segment_split, so the
+// result is bit-identical to the scan.
+template <int D, bool DENS, int NR, bool FAST>
+__device__ __forceinline__ void epoch_segment_split_bits(const EpochArgs &A, WarpSmem<D, kU> &S, float (*part)[32][D],
+                                                         unsigned *has_w, uint32_t *wm, uint32_t *pre,
+                                                         uint32_t node0, int warp, int lane)
+{
+    const uint32_t sbeg = A.offsets[node0], send = A.offsets[min(node0 + 32u, A.n)];
+    const uint32_t w0 = sbeg >> 5, nw = send > sbeg ? ((send - 1) >> 5) - w0 + 1 : 0;
+    if (nw > kSplitWords) {  // block-uniform
+        if (warp == 0) epoch_segment<D, DENS, NR, false, kU, FAST, false, true>(A, S, node0, lane);
+        return;
+    }
+    const uint32_t node = node0 + lane;
+    const bool valid = node < A.n;
+    float ys[D];
+    if (warp == 0) load_segment<D, DENS, false>(A, S, node0, lane, ys);
+    // masked words and their popcounts; exclusive prefix by warp 0
+    for (uint32_t t = threadIdx.x; t < nw; t += blockDim.x) {
+        const uint32_t wi = w0 + t;
+        uint32_t m = __ldg(A.bits + wi);
+        if (wi * 32u < sbeg) m &= ~0u << (sbeg - wi * 32u);
+        if (wi * 32u + 32u > send) m &= (send - wi * 32u >= 32u) ? ~0u : ((1u << (send - wi * 32u)) - 1u);
+        wm[t] = m;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t carry = 0;
+        for (uint32_t t0 = 0; t0 < nw; t0 += 32) {
+            const uint32_t t = t0 + lane;
+            const uint32_t c = t < nw ? __popc(wm[t]) : 0u;
+            uint32_t x = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(kFull, x, o);
+                if (lane >= o) x += y;
+            }
+            if (t < nw) pre[t] = carry + x - c;
+            carry += __shfl_sync(kFull, x, 31);
+        }
+        if (lane == 0) pre[kSplitWords] = carry;  // total active entries
+    }
+    __syncthreads();
+    const uint32_t total = pre[kSplitWords];
+    const float *dstat = A.dens_stats;
+    float g[D];
+#pragma unroll
+    for (int d = 0; d < D; d++) g[d] = 0.0f;
+    bool act = false;
+    for (uint32_t r0 = 0; r0 < total; r0 += 32u * kWarps) {  // block-uniform
+        const uint32_t rb = r0 + 32u * warp;
+        unsigned has = 0;
+        if (rb < total) {  // warp-uniform
+            const uint32_t r = rb + lane;
+            const bool live = r < total;
+            uint32_t p = 0, o = 0, j = 0, el = 0;
+            if (live) {
+                uint32_t lo = 0, hi = nw;  // last word with pre <= r
+                while (hi - lo > 1) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (pre[mid] <= r) lo = mid;
+                    else hi = mid;
+                }
+                p = (w0 + lo) * 32u + select_bit(wm[lo], r - pre[lo]);
+                o = __ldg(A.other + p);
+                j = local_node(S.beg, p);
+                el = p - S.beg[j];
+            }
+            float gd[D];
+            bool ad = false;
+            has = process_batch<D, DENS, NR, false, kU, FAST, true>(A, S, live, p, o, j, el, node0, lane, gd, ad,
+                                                                    dstat, part[warp]);
+        }
+        if (lane == 0) has_w[warp] = has;
+        __syncthreads();
+        if (warp == 0) {
+#pragma unroll
+            for (int w = 0; w < kWarps; w++) {
+                if ((has_w[w] >> lane) & 1u) {
+                    act = true;
+#pragma unroll
+                    for (int d = 0; d < D; d++) g[d] += part[w][lane][d];
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (warp != 0 || !valid) return;
+    finish_node<D, false>(A, node, ys, g, act);
+}
+
 }  // namespace umapcu

@@ -28,9 +28,10 @@
 //
 // With the schedule precomputed (schedule.cu) the kernel either scans the
 // epoch's active-entry bitmask in place of the (cursor, period) pairs (BITS),
-// or reads the epoch's active-entry records without any scan (LIST; a block
-// per segment on small problems, k_epoch_split). All three pick the same
-// entries in the same order, so their results are bit-identical.
+// or reads the epoch's active-entry records without any scan (LIST). On
+// small problems both give each segment a whole block (k_epoch_split_bits,
+// k_epoch_split). All pick the same entries in the same order and form the
+// same batches, so their results are bit-identical.
 //
 // Arithmetic follows the reference expression by expression with no FMA
 // contraction (compiled with -fmad=false). x^b is evaluated by pow_pos
@@ -63,6 +64,19 @@ __global__ void __launch_bounds__(kWarps * 32) k_epoch_split(const EpochArgs A)
     __shared__ unsigned has_w[kWarps];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     epoch_segment_split<D, DENS, NR, FAST>(A, seg, part, has_w, blockIdx.x * 32u, warp, lane);
+}
+
+// The bitmask form on a small problem: one block per segment, see
+// epoch_segment_split_bits.
+template <int D, bool DENS, int NR, bool FAST>
+__global__ void __launch_bounds__(kWarps * 32) k_epoch_split_bits(const EpochArgs A)
+{
+    __shared__ WarpSmem<D, kU> seg;
+    __shared__ float part[kWarps][32][D];
+    __shared__ unsigned has_w[kWarps];
+    __shared__ uint32_t wm[kSplitWords], pre[kSplitWords + 1];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    epoch_segment_split_bits<D, DENS, NR, FAST>(A, seg, part, has_w, wm, pre, blockIdx.x * 32u, warp, lane);
 }
 
 // ------------------------------------------------------------ densMAP
@@ -284,6 +298,10 @@ static void launch_epoch_t(const EpochArgs &A, cudaStream_t s)
         if (A.neg_rate == 5 && fast) k_epoch<D, DENS, 5, true, true><<<grid, kWarps * 32, 0, s>>>(A);
         else if (A.neg_rate == 5) k_epoch<D, DENS, 5, false, true><<<grid, kWarps * 32, 0, s>>>(A);
         else k_epoch<D, DENS, 0, false, true><<<grid, kWarps * 32, 0, s>>>(A);
+    } else if (A.bits && nseg < kSplitSegments) {
+        if (A.neg_rate == 5 && fast) k_epoch_split_bits<D, DENS, 5, true><<<nseg, kWarps * 32, 0, s>>>(A);
+        else if (A.neg_rate == 5) k_epoch_split_bits<D, DENS, 5, false><<<nseg, kWarps * 32, 0, s>>>(A);
+        else k_epoch_split_bits<D, DENS, 0, false><<<nseg, kWarps * 32, 0, s>>>(A);
     } else if (A.bits) {
         if (A.neg_rate == 5 && fast) k_epoch<D, DENS, 5, true, false, true><<<grid, kWarps * 32, 0, s>>>(A);
         else if (A.neg_rate == 5) k_epoch<D, DENS, 5, false, false, true><<<grid, kWarps * 32, 0, s>>>(A);

@@ -146,3 +146,32 @@ def test_one_shot_bitmask_equals_scan_densmap_3d():
     p = umapcu.UmapOptimParams(n_epochs=60)
     emb = init_embedding(2500, 3, seed=13)
     assert np.array_equal(_one_shot(adj, emb, p, dens), _one_shot(adj, emb, p, dens, precompute=False))
+
+
+def test_one_shot_bitmask_warp_per_segment_equals_scan():
+    import umapcu.synth as S
+    n = 60000  # above the block-per-segment threshold: the warp-per-segment bitmask scan
+    X, _ = S.isotropic_mixture(n, 20, 10, 4)
+    idx, dist = umapcu.knn_exact(X, 15)
+    adj = umapcu.coo_to_adjacency_list(umapcu.construct_umap_graph(idx, dist, umapcu.UmapGraphParams(), 40))
+    p = umapcu.UmapOptimParams(n_epochs=40)
+    emb = init_embedding(n, 2, seed=14)
+    assert np.array_equal(_one_shot(adj, emb, p), _one_shot(adj, emb, p, precompute=False))
+
+
+def test_one_shot_bitmask_hub_segment_equals_scan():
+    """A hub with 9000 neighbours puts more than 256 bitmask words into one
+    segment: that segment runs the sequential scan on one warp while the
+    others are shared by the block's warps; still bit-identical."""
+    import scipy.sparse as sp
+    g = oracle_graph(n=12000, dim=20, k=10, n_epochs=50)
+    n = 12000
+    A = sp.csr_matrix((g["val"].astype(np.float32), (g["row"], g["col"])), shape=(n, n))
+    hub = sp.csr_matrix((np.full(9000, 0.5, np.float32), (np.zeros(9000, np.int64), np.arange(1, 9001))),
+                        shape=(n, n))
+    A = A.maximum(hub).maximum(hub.T).tocsr()
+    A.sort_indices()
+    adj = umapcu.Adjacency(A.indptr.astype(np.uint64), A.indices.astype(np.uint32), A.data.astype(np.float32))
+    p = umapcu.UmapOptimParams(n_epochs=50)
+    emb = init_embedding(n, 2, seed=15)
+    assert np.array_equal(_one_shot(adj, emb, p), _one_shot(adj, emb, p, precompute=False))
