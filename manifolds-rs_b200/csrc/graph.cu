@@ -15,7 +15,9 @@
 // (the translation unit is compiled with -fmad=false). exp is evaluated as
 // (float)exp((double)x), i.e. correctly rounded except in double-rounding
 // corner cases; the reference calls glibc expf.
+#include <atomic>
 #include <cfloat>
+
 #include <cub/cub.cuh>
 
 #include "internal.cuh"
@@ -24,11 +26,13 @@ namespace umapcu {
 
 int device_sm_count()
 {
-    static int sms = 0;
+    static std::atomic<int> cached{0};  // the same value from every thread
+    int sms = cached.load(std::memory_order_relaxed);
     if (!sms) {
         int dev = 0;
         check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
         check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "sm count");
+        cached.store(sms, std::memory_order_relaxed);
     }
     return sms;
 }

@@ -269,17 +269,6 @@ __global__ void k_dens_final(const double2 *__restrict__ part, uint32_t nparts, 
 
 // ------------------------------------------------------------ launchers
 
-template <int D, bool DENS, int NR>
-static void set_carveout()
-{
-    static bool done = false;
-    if (!done) {
-        cudaFuncSetAttribute(k_epoch<D, DENS, NR>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                             cudaSharedmemCarveoutMaxShared);
-        done = true;
-    }
-}
-
 // Below this many segments (about 9 blocks of one warp per segment on each
 // of the 148 SMs) the list path gives each segment a whole block.
 constexpr uint32_t kSplitSegments = 148 * 9;

@@ -175,3 +175,29 @@ def test_one_shot_bitmask_hub_segment_equals_scan():
     p = umapcu.UmapOptimParams(n_epochs=50)
     emb = init_embedding(n, 2, seed=15)
     assert np.array_equal(_one_shot(adj, emb, p), _one_shot(adj, emb, p, precompute=False))
+
+
+def test_one_shot_concurrent_calls_share_the_bitmask_cache(prob):
+    """Four threads run the one-shot call at once (ctypes drops the GIL): one
+    takes the cached bitmask block, the others allocate their own, and every
+    result equals the same call run alone."""
+    import threading
+    g, adj = prob
+    p = umapcu.UmapOptimParams(n_epochs=40)
+    embs = [init_embedding(3000, 2, seed=20 + i) for i in range(4)]
+    alone = [_one_shot(adj, e, p, seed=30 + i) for i, e in enumerate(embs)]
+    outs = [None] * 4
+
+    def work(i):
+        y = np.ascontiguousarray(embs[i].copy())
+        umapcu.optimise_embedding_adam_gpu(y, adj, p, None, 30 + i, 0, umapcu.NEG_REF_HASH, umapcu.OPT_ADAM)
+        outs[i] = y
+
+    for _ in range(2):
+        ts = [threading.Thread(target=work, args=(i,)) for i in range(4)]
+        for t in ts:
+            t.start()
+        for t in ts:
+            t.join()
+        for i in range(4):
+            assert np.array_equal(outs[i], alone[i]), i
