@@ -263,6 +263,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--profile-only", action="store_true", help="a 40-epoch state, run once, for ncu captures")
+    ap.add_argument("--profile-one-shot", action="store_true",
+                    help="one 40-epoch one-shot call (per-epoch bitmasks), for ncu captures")
     ap.add_argument("--requests", type=int, default=0, help="served workload: number of requests")
     args = ap.parse_args()
 
@@ -299,6 +301,14 @@ def main():
     prob = make_problem(wl, seed)
     sampler = umapcu.NEG_PHILOX if args.sampler == "philox" else umapcu.NEG_REF_HASH
     opt = umapcu.OPT_SGD if args.optimiser == "sgd" else umapcu.OPT_ADAM
+    if args.profile_one_shot:
+        # the one-shot call's epoch kernel (bitmask scan) for ncu captures
+        import dataclasses
+        p40 = dataclasses.replace(prob["params"], n_epochs=min(wl["n_epochs"], 40))
+        y = np.ascontiguousarray(prob["init"].copy())
+        umapcu.optimise_embedding_adam_gpu(y, prob["adj"], p40, prob["dens"], seed, 0, sampler, opt)
+        log(f"[bench] profile-one-shot run done, finite {bool(np.isfinite(y).all())}")
+        return
     if args.profile_only:
         # a short run for ncu captures: a state made for 40 epochs (schedule
         # lists of 40 epochs, ~1/5 of the full run's device memory), run once
