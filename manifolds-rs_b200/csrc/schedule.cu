@@ -1,4 +1,6 @@
-// Per-epoch lists of active CSR entries ("schedule lists").
+// The edge schedule precomputed for a whole run, in two forms: per-epoch
+// lists of active CSR entries ("schedule lists", resident states) and
+// per-epoch bitmasks of them (the one-shot call).
 //
 // The edge schedule (umap_edge_schedule_update, umap_optimiser_gpu.rs:
 // 940-955) is a fixed function of each entry's period: the cursor starts at
@@ -18,6 +20,10 @@
 // counts and unit_base [nseg + 1] the segments' first units, so epoch e,
 // segment s owns rec[ptr[e * n_units + unit_base[s]] ..
 // ptr[e * n_units + unit_base[s + 1]]).
+//
+// Bitmasks: bits [n_epochs][ceil(2E / 32)], bit p & 31 of word p >> 5 set
+// when entry p is active in that epoch; the epoch kernel scans these words
+// in place of the (cursor, period) pairs.
 #include <chrono>
 #include <cstdlib>
 #include <mutex>
