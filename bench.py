@@ -572,7 +572,8 @@ def run_batched(args, wl, world, rank, local_rank):
            "sequential_plain": {"embeddings_per_s": P / t_seq, "ms": round(t_seq * 1e3, 3)},
            "speedup_vs_sequential": round((P / t_batch * args.steps) / (P / t_seq), 2) if t_seq > 0 else None,
            "same_result_alone_and_batched": ok,
-           "gpu_launches": args.steps * 2,
+           # per run: the state reset kernel, then one persistent launch or one launch per epoch
+           "gpu_launches": args.steps * (1 + (1 if cfg["mode"] == 1 else wl["n_epochs"])),
            "clocks": clk.summary()}
     if rank == 0:
         print(json.dumps(out), flush=True)

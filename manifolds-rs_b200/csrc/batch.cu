@@ -23,8 +23,15 @@
 // (the kernel boundary is the barrier), also captured in a graph. The
 // autotuner times both, with several CTA counts and super-chunk widths, on
 // the batch itself and keeps the fastest.
+//
+// With the reference hash sampler and neg_rate 5 (the fast kernels) the
+// batch precomputes each problem's schedule as per-epoch bitmasks at
+// creation (schedule.cu); the kernels scan those in place of the cursors,
+// which every run would otherwise stream and rewrite. Results are
+// bit-identical either way.
 #include <algorithm>
 #include <chrono>
+#include <cstdlib>
 #include <memory>
 #include <vector>
 
@@ -64,6 +71,8 @@ struct umapcu_batch {
     std::vector<DeviceCsr> csr;
     std::vector<DevBuf<float>> y0, y1, m, v, init;
     std::vector<DevBuf<float4>> scal;
+    std::vector<DevBuf<uint32_t>> bits;  // per-problem schedule bitmasks (when use_bits)
+    bool use_bits = false;
     std::vector<BatchProblem> hprobs;
     DevBuf<BatchProblem> probs;
     DevBuf<uint32_t> seg_prob;
@@ -124,9 +133,9 @@ void enqueue_run(umapcu_batch *b, const BatchConfig &c, uint32_t epochs, uint32_
     const uint32_t launches = c.mode == 1 ? 1 : epochs;
     for (uint32_t e = 0; e < launches; e++) {
         switch (b->n_dim) {
-            case 2: b->all_nr5 ? launch_batch_kernel<2>(B, c, s, e, b->sampler == UMAPCU_NEG_REF_HASH) : launch_batch_kernel_nr0<2>(B, c, s, e); break;
-            case 3: b->all_nr5 ? launch_batch_kernel<3>(B, c, s, e, b->sampler == UMAPCU_NEG_REF_HASH) : launch_batch_kernel_nr0<3>(B, c, s, e); break;
-            case 4: b->all_nr5 ? launch_batch_kernel<4>(B, c, s, e, b->sampler == UMAPCU_NEG_REF_HASH) : launch_batch_kernel_nr0<4>(B, c, s, e); break;
+            case 2: b->all_nr5 ? launch_batch_kernel<2>(B, c, s, e, b->sampler == UMAPCU_NEG_REF_HASH, b->use_bits) : launch_batch_kernel_nr0<2>(B, c, s, e); break;
+            case 3: b->all_nr5 ? launch_batch_kernel<3>(B, c, s, e, b->sampler == UMAPCU_NEG_REF_HASH, b->use_bits) : launch_batch_kernel_nr0<3>(B, c, s, e); break;
+            case 4: b->all_nr5 ? launch_batch_kernel<4>(B, c, s, e, b->sampler == UMAPCU_NEG_REF_HASH, b->use_bits) : launch_batch_kernel_nr0<4>(B, c, s, e); break;
             default: fail(UMAPCU_BAD_ARG, "batched n_dim must be 2, 3 or 4");
         }
     }
@@ -309,6 +318,27 @@ umapcu_status umapcu_batch_create(uint32_t n_problems, const uint32_t *n, uint32
             for (uint32_t k = 0; k < P.nseg; k++) seg_prob.push_back(p);
         }
         if ((uint64_t)seg_prob.size() * n_epochs >= (1ull << 32)) return UMAPCU_BAD_ARG;
+        // every run starts from the reset schedule and walks epochs 0, 1, ...
+        // in order, so the fast kernels can scan per-epoch bitmasks of the
+        // active entries in place of the cursors (bit-identical); skipped
+        // when they would take more than half the free device memory
+        if (b->all_nr5 && sampler == UMAPCU_NEG_REF_HASH && !getenv("UMAPCU_NO_SCHEDULE_LISTS")) {
+            uint64_t words_total = 0;
+            for (uint32_t p = 0; p < n_problems; p++) words_total += (b->hprobs[p].n_entries + 31) / 32;
+            size_t free_b = 0, total_b = 0;
+            check_cuda(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+            if (words_total * n_epochs * sizeof(uint32_t) <= free_b / 2) {
+                b->bits.resize(n_problems);
+                for (uint32_t p = 0; p < n_problems; p++) {
+                    BatchProblem &P = b->hprobs[p];
+                    P.bits_words = (P.n_entries + 31) / 32;
+                    b->bits[p].alloc((size_t)P.bits_words * n_epochs, s);
+                    launch_schedule_bits(b->csr[p].sched.p, P.n_entries, n_epochs, b->bits[p].p, s);
+                    P.bits = b->bits[p].p;
+                }
+                b->use_bits = true;
+            }
+        }
         b->n_segs = (uint32_t)seg_prob.size();
         b->probs.alloc(n_problems, s);
         h2d(b->probs.p, b->hprobs.data(), n_problems, s);

@@ -18,6 +18,8 @@ struct BatchProblem {
     float *y0, *y1, *m, *v;
     const float4 *scal;  // [n_epochs] {fused, epsc, lr_e, 0}
     const float *init;   // [n * n_dim] initial embedding (restored by every run)
+    const uint32_t *bits;  // [n_epochs][bits_words] schedule bitmasks (batched form), or nullptr
+    uint64_t bits_words;
     uint64_t n_entries;  // 2E
     float a, b, two_a_b, two_gamma_b, omb1, omb2;
     uint32_t neg_rate, sampler, seed32, seed_lo, seed_hi, pad1;
@@ -49,6 +51,7 @@ __device__ __forceinline__ void epoch_args_of(const BatchProblem &P, uint32_t e,
     A.offsets = P.offsets;
     A.other = P.other;
     A.sched = P.sched;
+    A.bits = P.bits ? P.bits + (size_t)e * P.bits_words : nullptr;
     A.y_cur = (e & 1) ? P.y1 : P.y0;
     A.y_next = (e & 1) ? P.y0 : P.y1;
     A.m = P.m;
@@ -74,7 +77,9 @@ __device__ __forceinline__ void epoch_args_of(const BatchProblem &P, uint32_t e,
     A.optimiser = optimiser;
 }
 
-template <int D, int NR, int KU, bool FAST = false>
+// BITS: every problem has its schedule bitmasks (P.bits), scanned in place of
+// the cursors.
+template <int D, int NR, int KU, bool FAST = false, bool BITS = false>
 __global__ void __launch_bounds__(kWarps * 32, 8) k_batch_persistent(const BatchArgs B)
 {
     __shared__ WarpSmem<D, KU> smem[kWarps];
@@ -112,7 +117,8 @@ __global__ void __launch_bounds__(kWarps * 32, 8) k_batch_persistent(const Batch
                 sargs[warp] = A;
             }
             __syncwarp();
-            epoch_segment<D, false, NR, true, KU, FAST>(sargs[warp], smem[warp], (s - P.seg_base) * 32u, lane);
+            epoch_segment<D, false, NR, true, KU, FAST, false, BITS>(sargs[warp], smem[warp], (s - P.seg_base) * 32u,
+                                                                     lane);
         }
         __threadfence();
         __syncwarp();
@@ -120,7 +126,7 @@ __global__ void __launch_bounds__(kWarps * 32, 8) k_batch_persistent(const Batch
     }
 }
 
-template <int D, int NR, int KU, bool FAST = false>
+template <int D, int NR, int KU, bool FAST = false, bool BITS = false>
 __global__ void __launch_bounds__(kWarps * 32, 8) k_batch_epoch(const BatchArgs B, uint32_t e)
 {
     __shared__ WarpSmem<D, KU> smem[kWarps];
@@ -137,7 +143,7 @@ __global__ void __launch_bounds__(kWarps * 32, 8) k_batch_epoch(const BatchArgs 
         sargs[warp] = A;
     }
     __syncwarp();
-    epoch_segment<D, false, NR, false, KU, FAST>(sargs[warp], smem[warp], (s - P.seg_base) * 32u, lane);
+    epoch_segment<D, false, NR, false, KU, FAST, false, BITS>(sargs[warp], smem[warp], (s - P.seg_base) * 32u, lane);
 }
 
 struct BatchConfig {
@@ -149,27 +155,30 @@ struct BatchConfig {
 // fast: every problem uses the reference hash sampler (the batched and served
 // forms have no injected negatives and no precise mode), so the kernels can
 // take the compile-time fast path.
-template <int D, bool FAST>
+template <int D, bool FAST, bool BITS>
 inline void launch_batch_kernel_t(const BatchArgs &B, const BatchConfig &c, cudaStream_t s, uint32_t epoch)
 {
     if (c.mode == 1) {
         const unsigned grid = (unsigned)(c.ctas_per_sm * device_sm_count());
-        if (c.ku == 4) k_batch_persistent<D, 5, 4, FAST><<<grid, kWarps * 32, 0, s>>>(B);
-        else k_batch_persistent<D, 5, 8, FAST><<<grid, kWarps * 32, 0, s>>>(B);
+        if (c.ku == 4) k_batch_persistent<D, 5, 4, FAST, BITS><<<grid, kWarps * 32, 0, s>>>(B);
+        else k_batch_persistent<D, 5, 8, FAST, BITS><<<grid, kWarps * 32, 0, s>>>(B);
     } else {
         const unsigned grid = ceil_div(B.n_segs, kWarps);
-        if (c.ku == 4) k_batch_epoch<D, 5, 4, FAST><<<grid, kWarps * 32, 0, s>>>(B, epoch);
-        else k_batch_epoch<D, 5, 8, FAST><<<grid, kWarps * 32, 0, s>>>(B, epoch);
+        if (c.ku == 4) k_batch_epoch<D, 5, 4, FAST, BITS><<<grid, kWarps * 32, 0, s>>>(B, epoch);
+        else k_batch_epoch<D, 5, 8, FAST, BITS><<<grid, kWarps * 32, 0, s>>>(B, epoch);
     }
     check_launch("k_batch");
 }
 
+// bits: every problem carries its schedule bitmasks (the batched form; the
+// served form scans the cursors)
 template <int D>
 inline void launch_batch_kernel(const BatchArgs &B, const BatchConfig &c, cudaStream_t s, uint32_t epoch,
-                                bool fast)
+                                bool fast, bool bits = false)
 {
-    if (fast) launch_batch_kernel_t<D, true>(B, c, s, epoch);
-    else launch_batch_kernel_t<D, false>(B, c, s, epoch);
+    if (fast && bits) launch_batch_kernel_t<D, true, true>(B, c, s, epoch);
+    else if (fast) launch_batch_kernel_t<D, true, false>(B, c, s, epoch);
+    else launch_batch_kernel_t<D, false, false>(B, c, s, epoch);
 }
 
 template <int D>

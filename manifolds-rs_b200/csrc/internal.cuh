@@ -239,6 +239,10 @@ struct ScheduleBits {
 // false when they would not fit (half the free device memory), `out` then
 // empty.
 bool build_schedule_bits(const DeviceCsr &csr, uint32_t n_epochs, ScheduleBits &out, cudaStream_t s);
+// The bitmask kernel alone: bits [n_epochs][ceil(n_entries / 32)] of the
+// entries' reset schedule (sched[p].y = period), into caller memory.
+void launch_schedule_bits(const float2 *sched, uint64_t n_entries, uint32_t n_epochs, uint32_t *bits,
+                          cudaStream_t s);
 
 // Writes into csr.sched the cursors after `epochs` epochs from the reset
 // schedule (the state the per-epoch scan would have left).

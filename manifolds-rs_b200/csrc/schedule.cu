@@ -293,6 +293,15 @@ ScheduleBits::~ScheduleBits()
     }
 }
 
+void launch_schedule_bits(const float2 *sched, uint64_t n_entries, uint32_t n_epochs, uint32_t *bits,
+                          cudaStream_t s)
+{
+    const uint64_t words = (n_entries + 31) / 32;
+    if (!words || !n_epochs) return;
+    k_sched_bits<<<ceil_div(words, 128), 128, 0, s>>>(sched, n_entries, words, n_epochs, bits);
+    check_launch("k_sched_bits");
+}
+
 bool build_schedule_bits(const DeviceCsr &csr, uint32_t n_epochs, ScheduleBits &out, cudaStream_t s)
 {
     const uint64_t entries = 2 * csr.n_edges;
@@ -326,8 +335,7 @@ bool build_schedule_bits(const DeviceCsr &csr, uint32_t n_epochs, ScheduleBits &
     out.cap = blk.cap;
     out.dev = dev;
     out.built_on = s;
-    k_sched_bits<<<ceil_div(words, 128), 128, 0, s>>>(csr.sched.p, entries, words, n_epochs, out.bits);
-    check_launch("k_sched_bits");
+    launch_schedule_bits(csr.sched.p, entries, n_epochs, out.bits, s);
     out.words = words;
     out.n_epochs = n_epochs;
     return true;
