@@ -223,7 +223,12 @@ umapcu_status umapcu_state_dens_update(umapcu_state *st, float *re, float *phi_s
 typedef struct umapcu_batch umapcu_batch;
 
 /* Uploads every problem and builds its CSR on the device. Arrays of
- * n_problems pointers / values; params and seeds per problem. */
+ * n_problems pointers / values; params and seeds per problem. With the
+ * hash sampler and neg_sample_rate 5 everywhere it also precomputes each
+ * problem's edge schedule as per-epoch bitmasks (1 bit per CSR entry and
+ * epoch, held until umapcu_batch_destroy; not when they would take more
+ * than half the free device memory, nor with UMAPCU_NO_SCHEDULE_LISTS set),
+ * which the runs scan in place of the cursors with identical results. */
 umapcu_status umapcu_batch_create(uint32_t n_problems, const uint32_t *n, uint32_t n_dim,
                                   const float *const *embd, const uint64_t *const *adj_ptr,
                                   const uint32_t *const *adj_col, const float *const *adj_w,
