@@ -40,6 +40,19 @@ METRIC = "UMAP layout edge-updates/s (1M pts)"
 UNIT = "edge-updates/s"
 
 
+def max_over_ranks(x, dist):
+    """x maximised over the ranks of dist's default group, or x itself
+    without one; the tensor lives where the group's backend wants it (CUDA
+    for NCCL, host memory for gloo)."""
+    if dist is None:
+        return float(x)
+    import torch
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def metric_of(wl):
     """The headline metric's name for the 1M-point layout; the other layout
     workloads name their own size."""
@@ -365,18 +378,10 @@ def main():
         st2.set_stream(stream.cuda_stream)
         st2.reset(prob["init"])
         st2.run(0, n_ep, opt)
-        t2 = float(np.sum(time_steps(st2)))
-        if dist:
-            tt = torch.tensor([t2], device="cuda", dtype=torch.float64)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            t2 = float(tt.item())
+        t2 = max_over_ranks(np.sum(time_steps(st2)), dist)
         scan_value = world * args.steps * updates_per_step / t2
         st2.close()
-    total = float(np.sum(times))
-    if dist:
-        t = torch.tensor([total], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total = float(t.item())
+    total = max_over_ranks(np.sum(times), dist)
     value = world * args.steps * updates_per_step / total
     ms_per_step = total / args.steps * 1e3
 
@@ -430,11 +435,7 @@ def main():
             t0 = time.perf_counter()
             umapcu.optimise_embedding_adam_gpu(embd_p, A, prob["params"], prob["dens"], seed, 0, sampler, opt)
             tt.append(time.perf_counter() - t0)
-        et = float(np.sum(tt))
-        if dist:
-            t = torch.tensor([et], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            et = float(t.item())
+        et = max_over_ranks(np.sum(tt), dist)
         h2d = ptr_p.nbytes + col_p.nbytes + w_p.nbytes + embd_p.nbytes
         e2e = {"value": world * e2e_steps * updates_per_step / et, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(embd_p.nbytes), "ms_per_step": round(et / e2e_steps * 1e3, 3)}
