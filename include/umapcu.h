@@ -304,25 +304,33 @@ void umapcu_server_destroy(umapcu_server *sv);
 
 /* Layout optimisation that allocates no device memory. No counterpart in
  * the reference: for callers that cannot allocate device memory when they
- * need a layout (inside a stream callback or host function node, under a
- * framework that has reserved the device for its own allocator, or with a
- * device-memory budget fixed at start-up). Runs all params->n_epochs Adam
- * epochs (plain UMAP, no densMAP) of the same fused epoch kernel as
- * umapcu_optimise_embedding on the caller's stream (a cudaStream_t passed
- * as void*, NULL = legacy default stream); returns once the work is
- * enqueued. Inputs and outputs are device memory owned by the caller:
- * d_embd [n * n_dim] (in/out), the optimiser CSR d_offsets [n + 1],
- * d_other and d_period [n_entries] (per CSR entry: other endpoint and edge
- * sampling period, as umapcu_state_read_csr returns them, periods expanded
- * per entry through edge_idx). All scratch (Adam moments, the second
- * embedding buffer, schedule cursors) lives in one 16 MiB device array that
- * every GPU loading the library holds until exit: a call needs
- * 8 * n_entries + 12 * n * n_dim bytes (each part rounded up to 256) and
- * larger problems return UMAPCU_CAPACITY. The array is shared by every call
- * on a device and keeps the last call's contents (each call re-initialises
- * what it reads); calls that overlap on the GPU race on it. The first call on
- * a device looks the array's device address up (cudaGetSymbolAddress); make
- * that first call before any stream capture. */
+ * need a layout (a host framework that has reserved the device for its own
+ * allocator, or a deployment whose device-memory budget is fixed at
+ * start-up). It is an ordinary host call (it makes CUDA runtime calls): never
+ * call it from a stream callback or a host function node, where CUDA forbids
+ * runtime calls. Runs all params->n_epochs Adam epochs (plain UMAP, no
+ * densMAP) of the same fused epoch kernel as umapcu_optimise_embedding on
+ * the caller's stream (a cudaStream_t passed as void*, NULL = legacy default
+ * stream); returns once the work is enqueued. Inputs and outputs are device
+ * memory owned by the caller: d_embd [n * n_dim] (in/out; 8-byte aligned for
+ * n_dim = 2, 16-byte aligned for n_dim = 4, 4-byte aligned otherwise), the
+ * optimiser CSR d_offsets [n + 1], d_other and d_period [n_entries] (4-byte
+ * aligned; per CSR entry: other endpoint and edge sampling period, as
+ * umapcu_state_read_csr returns them, periods expanded per entry through
+ * edge_idx). A misaligned pointer returns UMAPCU_BAD_ARG before anything is
+ * launched. All scratch (Adam moments, the second embedding buffer,
+ * schedule cursors) lives in one 16 MiB device array that every GPU loading
+ * the library holds until exit: a call needs 8 * n_entries + 12 * n * n_dim
+ * bytes (each part rounded up to 256) and larger problems return
+ * UMAPCU_CAPACITY. The array is shared by every call on a device and keeps
+ * the last call's contents (each call re-initialises what it reads); calls
+ * that overlap on the GPU race on it. The first call on a device looks the
+ * array's device address up (cudaGetSymbolAddress) and, under CUDA's default
+ * lazy module loading, is also when the library's device code and this
+ * array are loaded onto that device, which takes device memory: make one
+ * call per device at start-up, before the caller reserves the device's
+ * memory and before any stream capture (or run with
+ * CUDA_MODULE_LOADING=EAGER). */
 umapcu_status umapcu_optimise_csr_noalloc(float *d_embd, uint32_t n, uint32_t n_dim,
                                           const uint32_t *d_offsets, const uint32_t *d_other,
                                           const float *d_period, uint64_t n_entries,

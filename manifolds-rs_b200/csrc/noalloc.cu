@@ -1,14 +1,16 @@
 // Layout optimisation that allocates no device memory.
 //
 // Some callers cannot allocate device memory at the moment they want a
-// layout: code running where CUDA allocation calls are not allowed (a stream
-// callback, a host function node), a host framework that has reserved the
-// whole device for its own allocator, or a deployment whose device-memory
-// budget is fixed at start-up. For them, umapcu_optimise_csr_noalloc runs the
-// same fused epoch kernel as the allocating entry points, with every scratch
-// buffer (Adam moments, the second embedding buffer, the per-entry schedule
-// cursors) carved out of one file-scope device array of fixed size that the
-// library holds on every GPU that loads it, until the process exits.
+// layout: a host framework that has reserved the whole device for its own
+// allocator, or a deployment whose device-memory budget is fixed at start-up.
+// For them, umapcu_optimise_csr_noalloc runs the same fused epoch kernel as
+// the allocating entry points, with every scratch buffer (Adam moments, the
+// second embedding buffer, the per-entry schedule cursors) carved out of one
+// file-scope device array of fixed size that the library holds on every GPU
+// that loads it, until the process exits. It is an ordinary host call: it
+// makes CUDA runtime calls (device query, symbol lookup, memset, launches,
+// copy), so it must not be called from a stream callback or a host function
+// node, where CUDA forbids runtime calls.
 #include "internal.cuh"
 #include "layout.cuh"
 
@@ -67,6 +69,14 @@ extern "C" umapcu_status umapcu_optimise_csr_noalloc(float *d_embd, uint32_t n, 
         if (n_entries == 0) return UMAPCU_NO_GRAPH_EDGES;
         if (!d_embd || !d_offsets || !d_other || !d_period || !params) return UMAPCU_BAD_ARG;
         if (n_dim < 1 || n_dim > 8 || params->n_epochs == 0 || sampler > UMAPCU_NEG_PHILOX) return UMAPCU_BAD_ARG;
+        // The epoch kernel moves a row of the embedding (and of the moments)
+        // as one float2 for n_dim = 2 and one float4 for n_dim = 4, and reads
+        // the CSR arrays as 32-bit words: refuse pointers those accesses
+        // would fault on, before anything is launched.
+        const uintptr_t row_align = n_dim == 2 ? 8 : n_dim == 4 ? 16 : 4;
+        if ((uintptr_t)d_embd % row_align || (uintptr_t)d_offsets % 4 || (uintptr_t)d_other % 4 ||
+            (uintptr_t)d_period % 4)
+            return UMAPCU_BAD_ARG;
         const uint64_t nt = (uint64_t)n * n_dim;
         const size_t b_sched = round256(n_entries * sizeof(float2));
         const size_t b_vec = round256(nt * sizeof(float));

@@ -87,3 +87,23 @@ def test_bad_args_rejected_without_gpu():
         umapcu.optimise_embedding_adam_gpu(np.zeros((0, 2), np.float32), [], umapcu.UmapOptimParams())
     with pytest.raises(umapcu.ManifoldsError):
         umapcu.optimise_embedding_adam_gpu(np.zeros((3, 2), np.float64), [[], [], []], umapcu.UmapOptimParams())
+
+
+def test_noalloc_rejects_misaligned_pointers():
+    """umapcu_optimise_csr_noalloc refuses device pointers its float2 / float4
+    row accesses would fault on, before any CUDA call (so this runs without
+    a GPU): the embedding must be 8-byte aligned for n_dim = 2, 16-byte
+    aligned for n_dim = 4, the CSR arrays 4-byte aligned."""
+    import umapcu
+    fn = umapcu.lib().umapcu_optimise_csr_noalloc
+    fn.restype = C.c_int
+    fn.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64,
+                   C.c_void_p, C.c_uint64, C.c_uint32, C.c_void_p]
+    cp = umapcu.UmapOptimParams(n_epochs=10)._c()
+    good = 1 << 20
+    cases = [(good + 4, 2, good, good, good), (good + 8, 4, good, good, good), (good + 2, 3, good, good, good),
+             (good, 2, good + 2, good, good), (good, 2, good, good + 1, good), (good, 2, good, good, good + 3)]
+    for y, d, off, oth, per in cases:
+        rc = fn(C.c_void_p(y), 100, d, C.c_void_p(off), C.c_void_p(oth), C.c_void_p(per), 600, C.byref(cp), 1, 0,
+                None)
+        assert rc == umapcu.BAD_ARG, (y, d, off, oth, per, rc)
