@@ -4,9 +4,10 @@ Callers that cannot allocate device memory when they need a layout -- under
 a framework that has reserved the device for its own allocator, or with a
 device-memory budget fixed at start-up -- use this entry point: its scratch
 lives in a fixed device array inside the library. These checks call it
-through the C ABI with device buffers the test owns, and compare its embedding with the allocating entry point's
-(umapcu_optimise_embedding) on the same graph, initial embedding and seed,
-twice in a row (the second call finds the first call's scratch contents).
+through the C ABI with device buffers the test owns, and compare its
+embedding with the allocating entry point's (umapcu_optimise_embedding) on
+the same graph, initial embedding and seed, twice in a row (the second call
+finds the first call's scratch contents).
 
 This file is collected last so that a run which stops at the first failure
 has already run every other test.
