@@ -2,20 +2,32 @@
 """UMAP layout throughput on B200: edge-updates/s at 1M points.
 
 One step = one full layout run (all epochs) of one embedding problem from its
-cached fuzzy graph, the unit the reference's timing harness isolates
+fuzzy graph, the unit the reference's timing harness isolates
 (tests/umap_gpu_bench.rs:217-252). An edge-update is one active undirected
 edge in one epoch (cursor <= epoch), both endpoints' attractive and negative
 terms included; the count per epoch depends only on the edge periods, so it
 is the same for every implementation.
 
-  value  : device-resident state (graph, embedding, moments on the GPU),
-           CUDA events around the epoch loop on the launching stream,
-           L2 flushed (256 MiB write) before every step.
+  value  : device-resident graph and embedding; each timed step starts from
+           the reset state with L2 flushed (256 MiB write) and contains the
+           build of the run's schedule bitmasks and every epoch (CUDA events
+           on the launching stream). The other schedule forms (record lists
+           built in the step, plain cursor scan) are reported beside it.
   e2e    : the reference-facing call umapcu.optimise_embedding_adam_gpu
            (C ABI umapcu_optimise_embedding) from pinned host buffers:
-           H2D of graph + embedding, CSR build, epochs, D2H of the embedding.
-  --impl reference : the reference's parallel Adam (umap_optimisers.rs:
-           1170-1492, restated in oracle/) on the host cores, bounded windows.
+           H2D of graph + embedding, CSR build, bitmasks, epochs, D2H.
+  roofline: the fused epoch kernel's time per epoch from the timed region,
+           algorithmic HBM bytes against the measured copy bandwidth, and
+           its random coordinate gathers against the measured L2 gather rate.
+  cpu_baseline / --impl reference : the reference's parallel Adam
+           (umap_optimisers.rs:1170-1492, restated in oracle/) on all host
+           cores, whole runs from the initial embedding, epoch loop only.
+           The reference arm loads no umapcu code: its inputs come from
+           umapdata (NumPy) and the oracle.
+
+Both arms share one input: the workload's brute-force kNN, cached in a kNN
+cache file by whichever arm runs first (torch on the GPU, outside every timed
+region).
 
 Multi-GPU (torchrun): every rank runs its own problem (replicas, seed +
 rank); value is the sum over ranks / max-over-ranks time ("weak").
@@ -97,68 +109,98 @@ def log(*a):
 def knn_cache_path(wl, seed):
     d = os.environ.get("UMAPCU_KNN_CACHE") or os.path.join(__import__("tempfile").gettempdir(), "umapcu_knn")
     os.makedirs(d, exist_ok=True)
-    return os.path.join(d, f"{wl['kind']}_n{wl['n']}_d{wl['dim']}_c{wl['clusters']}_k{wl['k']}_s{seed}.knn")
+    return os.path.join(d, f"{wl['kind']}_n{wl['n']}_d{wl['dim']}_c{wl['clusters']}_k{wl['k']}_s{seed}_bf.knn")
 
 
 def shared_knn(X, wl, seed):
-    """The workload's exact kNN, computed once and cached (kNN cache file)
-    as the shared input of both arms: input preparation, outside every timed
-    region. Computed by the library's exact GPU kNN when a GPU is present,
-    else by the CPU brute force; both are exact (ties by index)."""
-    import umapcu
+    """The workload's brute-force kNN, computed once and cached (kNN cache
+    file) as the shared input of both arms: input preparation, outside every
+    timed region. Read and written with the NumPy reader of the cache format
+    and computed with torch (fp32 GEMM candidates, f64 distances of the
+    candidates) on the GPU, or NumPy without one, so that neither arm needs
+    the umapcu library to prepare it."""
+    from umapdata import knn_cache
+    import umapdata.synth as S
     path = knn_cache_path(wl, seed)
     if os.path.exists(path):
         try:
-            idx, dist, _ = umapcu.load_knn(path)
+            idx, dist, _ = knn_cache.load(path)
             if idx.shape == (wl["n"], wl["k"]):
                 log(f"[bench] kNN from cache {path}")
                 return idx, dist
-        except umapcu.ManifoldsError:
+        except ValueError:
             pass
     import torch
     if torch.cuda.is_available():
-        idx, dist = umapcu.knn_exact(X, wl["k"])
+        idx, dist = S.exact_knn_torch(X, wl["k"])
     else:
-        import umapcu.synth as S
         idx, dist = S.exact_knn_cpu(X, wl["k"])
-        idx, dist = idx.astype(np.int32), dist.astype(np.float32)
+    idx, dist = idx.astype(np.int32), dist.astype(np.float32)
     tmp = f"{path}.{os.getpid()}.tmp"
-    umapcu.save_knn(tmp, idx, dist)
+    knn_cache.save(tmp, idx, dist)
     os.replace(tmp, path)
     return idx, dist
 
 
-def make_problem(wl, seed, reference_graph=False):
-    """Synthetic data -> exact kNN (shared cached input) -> fuzzy graph: the
-    CUDA graph stage for the umapcu arm, the oracle's CPU restatement of the
-    reference's graph stage for the reference arm."""
-    import umapcu
-    import umapcu.synth as S
-    t0 = time.time()
+def make_data(wl, seed):
+    import umapdata.synth as S
     if wl["kind"] == "anisotropic":
-        X, _ = S.anisotropic_mixture(wl["n"], wl["dim"], wl["clusters"], seed)
-    elif wl["kind"] == "variable":
-        X, _ = S.variable_density_mixture(wl["n"], wl["dim"], wl["clusters"], seed)
-    else:
-        X, _ = S.isotropic_mixture(wl["n"], wl["dim"], wl["clusters"], seed)
+        return S.anisotropic_mixture(wl["n"], wl["dim"], wl["clusters"], seed)[0]
+    if wl["kind"] == "variable":
+        return S.variable_density_mixture(wl["n"], wl["dim"], wl["clusters"], seed)[0]
+    return S.isotropic_mixture(wl["n"], wl["dim"], wl["clusters"], seed)[0]
+
+
+def make_problem(wl, seed):
+    """Synthetic data -> shared cached kNN -> the CUDA graph stage (umapcu
+    arm)."""
+    import umapcu
+    import umapdata.synth as S
+    t0 = time.time()
+    X = make_data(wl, seed)
     idx, dist = shared_knn(X, wl, seed)
     t1 = time.time()
-    if reference_graph:
-        from oracle import oracle as O
-        (r, c, v), _, _ = O.construct_umap_graph(idx, dist, wl["n_epochs"])
-        graph = umapcu.CoordinateList(r, c, v, wl["n"])
-        dens = None
-        if wl["dens"]:
-            stt, d = O.dens_state_new(wl["n"], r, c, v, idx, dist, True)
-            dens = umapcu.DensState(umapcu.DensParams(), d["r"], d["mu_sum"], float(d["mu_tot"]))
-    else:
-        graph = umapcu.construct_umap_graph(idx, dist, umapcu.UmapGraphParams(), wl["n_epochs"])
-        dens = umapcu.DensState.new(umapcu.DensParams(), graph, idx, dist, True) if wl["dens"] else None
+    graph = umapcu.construct_umap_graph(idx, dist, umapcu.UmapGraphParams(), wl["n_epochs"])
+    dens = umapcu.DensState.new(umapcu.DensParams(), graph, idx, dist, True) if wl["dens"] else None
     adj = umapcu.coo_to_adjacency_list(graph)
     params = umapcu.UmapOptimParams.from_min_dist_spread(0.1, 1.0, n_epochs=wl["n_epochs"], neg_sample_rate=5)
-    init = umapcu.random_layout(wl["n"], 2, seed)
+    init = S.random_layout(wl["n"], 2, seed)
     log(f"[bench] data+kNN {t1 - t0:.1f}s, graph {time.time() - t1:.1f}s, nnz {adj.col.size}")
     return dict(X=X, idx=idx, dist=dist, graph=graph, adj=adj, dens=dens, params=params, init=init)
+
+
+def make_reference_problem(wl, seed):
+    """The same inputs for the reference arm, prepared without the umapcu
+    library: the oracle's CPU restatement of the reference's graph stage
+    (graph.rs:499-853), its densMAP state (density.rs:181-201) and its a, b
+    fit (umap_optimisers.rs:139-209)."""
+    import umapdata.synth as S
+    from oracle import oracle as O
+    t0 = time.time()
+    X = make_data(wl, seed)
+    idx, dist = shared_knn(X, wl, seed)
+    t1 = time.time()
+    (r, c, v), _, _ = O.construct_umap_graph(idx, dist, wl["n_epochs"])
+    ptr = O.coo_to_adj_ptr(wl["n"], r)
+    dens = None
+    if wl["dens"]:
+        _, d = O.dens_state_new(wl["n"], r, c, v, idx, dist, True)
+        dens = {"r": d["r"], "lambda": d["lambda"], "frac": d["frac"], "var_shift": d["var_shift"],
+                "mu_tot": d["mu_tot"]}
+    a, b = O.fit_params(0.1, 1.0)
+    params = dict(a=float(a), b=float(b), lr=1.0, gamma=1.0, n_epochs=wl["n_epochs"], neg_sample_rate=5,
+                  min_dist=0.1, beta1=0.5, beta2=0.9, eps=1e-7)
+    init = S.random_layout(wl["n"], 2, seed)
+    log(f"[bench] data+kNN {t1 - t0:.1f}s, oracle graph {time.time() - t1:.1f}s, nnz {c.size}")
+    return dict(ptr=ptr, col=c, w=v, dens=dens, params=params, init=init)
+
+
+def config_of(args, wl):
+    """The workload description both arms print (identical by construction)."""
+    return {"workload": f"{args.workload}: {wl['desc']}", "n_points": wl["n"], "k": wl["k"],
+            "epochs": wl["n_epochs"], "optimiser": args.optimiser, "neg_sample_rate": 5,
+            "l2": "GPU arm: L2 flushed (256 MiB write) before every timed step; CPU arm: no device",
+            "parallelism": f"replicas x{int(os.environ.get('WORLD_SIZE', '1'))}"}
 
 
 def active_edges_per_epoch(eps, n_epochs):
@@ -234,30 +276,20 @@ class ClockSampler:
 
 # ----------------------------------------------------------------- CPU leg
 
-def cpu_windows(prob, wl, seed, target_s, n_threads):
-    """Times the oracle's adam_parallel on bounded mid-run windows of the
-    same workload; returns (edge-updates/s, sample description, cores)."""
+def cpu_full_runs(ptr, col, w, params, init, dens, seed, reps, threads, n_epochs):
+    """Times whole runs of the oracle's adam_parallel (the reference's
+    optimise_embedding_adam_parallel, umap_optimisers.rs:1170-1492) from the
+    initial embedding: epoch loop only, as tests/umap_gpu_bench.rs:232-252
+    times it. Returns the loop seconds of each run."""
     from oracle import oracle as O
-    p = prob["params"].as_dict()
-    adj = prob["adj"]
-    dens = None
-    if prob["dens"] is not None:
-        d = prob["dens"]
-        dens = {"r": d.r, "lambda": d.params.lambda_, "frac": d.params.frac, "var_shift": d.params.var_shift,
-                "mu_tot": d.mu_tot}
-    n = wl["n"]
-    ae = prob["A_e"]
-    first = wl["n_epochs"] // 2
-    # calibrate on one epoch, then size the window to ~target_s
-    st, _, s1 = O.optimise_adam_parallel(prob["init"], n, adj.ptr, adj.col, adj.w, p, seed, dens, n_threads, 1,
-                                         first, True)
-    per = max(s1, 1e-3)
-    cnt = int(max(1, min(wl["n_epochs"] - first, round(target_s / per))))
-    st, _, secs = O.optimise_adam_parallel(prob["init"], n, adj.ptr, adj.col, adj.w, p, seed, dens, n_threads, cnt,
-                                           first, True)
-    updates = int(ae[first:first + cnt].sum())
-    return updates / secs, f"epochs {first}..{first + cnt - 1} of the {wl['n_epochs']}-epoch run " \
-                           f"({updates} edge-updates, {secs:.2f}s)", secs
+    n = init.shape[0]
+    out = []
+    for _ in range(reps):
+        st, _, secs = O.optimise_adam_parallel(init, n, ptr, col, w, params, seed, dens, threads, 0, 0, True)
+        if st != O.OK:
+            raise RuntimeError(f"oracle adam_parallel status {st}")
+        out.append(secs)
+    return out
 
 
 # ----------------------------------------------------------------- main
@@ -303,11 +335,7 @@ def main():
         return
 
     torch.cuda.set_device(local_rank)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    dist = init_group(world)
 
     import umapcu
     seed = args.seed + rank
@@ -337,81 +365,97 @@ def main():
     E = st.n_edges
     csr = st.csr()
     ae = active_edges_per_epoch(csr["eps"], wl["n_epochs"])
-    prob["A_e"] = ae
     updates_per_step = int(ae.sum())
     n_ep = wl["n_epochs"]
     stream = torch.cuda.current_stream()
     st.set_stream(stream.cuda_stream)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > L2
 
-    for _ in range(args.warmup):
-        st.reset(prob["init"])
-        st.run(0, n_ep, opt)
-    torch.cuda.synchronize()
-
-    def time_steps(state):
-        out = []
-        for _ in range(args.steps):
-            state.reset(prob["init"])
+    def time_steps(form, count):
+        """count steps of the whole layout: each from the reset state (input
+        embedding in HBM, moments zero, cursors at their periods) and a
+        flushed L2, the schedule's precomputed form built inside the timed
+        region, then every epoch. -> (step seconds, epoch-loop seconds)."""
+        tot, loop = [], []
+        for _ in range(count):
+            st.set_schedule(umapcu.SCHED_SCAN)  # frees the previous step's form (outside the region)
+            st.reset(prob["init"])
             flush.fill_(1.0)
             torch.cuda.synchronize()
             if dist:
                 dist.barrier()
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
+            e0, em, e1 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
             e0.record(stream)
-            state.run(0, n_ep, opt)
+            if form != umapcu.SCHED_SCAN:
+                st.set_schedule(form)
+            em.record(stream)
+            st.enqueue(0, n_ep, opt)
             e1.record(stream)
             torch.cuda.synchronize()
-            out.append(e0.elapsed_time(e1) / 1e3)
-        return out
+            tot.append(e0.elapsed_time(e1) / 1e3)
+            loop.append(em.elapsed_time(e1) / 1e3)
+        return tot, loop
 
+    time_steps(umapcu.SCHED_BITS, args.warmup)
     with ClockSampler(local_rank) as clk:
-        times = time_steps(st)
-    sched = st.schedule_info()
-    scan_value = None
-    if sched["lists"]:
-        # the same steps on a state that scans the CSR every epoch
-        os.environ["UMAPCU_NO_SCHEDULE_LISTS"] = "1"
-        st2 = umapcu.UmapGpuState(prob["init"], prob["adj"], prob["params"], prob["dens"], seed, sampler)
-        del os.environ["UMAPCU_NO_SCHEDULE_LISTS"]
-        st2.set_stream(stream.cuda_stream)
-        st2.reset(prob["init"])
-        st2.run(0, n_ep, opt)
-        t2 = max_over_ranks(np.sum(time_steps(st2)), dist)
-        scan_value = world * args.steps * updates_per_step / t2
-        st2.close()
+        times, loops = time_steps(umapcu.SCHED_BITS, args.steps)
     total = max_over_ranks(np.sum(times), dist)
     value = world * args.steps * updates_per_step / total
     ms_per_step = total / args.steps * 1e3
+    # the other schedule forms, same steps (secondary figures)
+    variants = {}
+    for name, form in (("lists", umapcu.SCHED_LISTS), ("csr_scan", umapcu.SCHED_SCAN)):
+        time_steps(form, 1)
+        t = max_over_ranks(np.sum(time_steps(form, args.steps)[0]), dist)
+        variants[name] = {"value": world * args.steps * updates_per_step / t,
+                          "ms_per_step": round(t / args.steps * 1e3, 3)}
+    variants["lists"]["note"] = "per-epoch record lists, built inside every timed step"
+    variants["csr_scan"]["note"] = "no precomputed schedule: every epoch scans and advances the cursors"
 
-    # roofline of the dominant kernel (fused epoch kernel), events per launch
-    st.reset(prob["init"])
-    torch.cuda.synchronize()
-    k_ms, d_ms = st.run_profiled(0, n_ep, opt)
-    avg_launch_s = k_ms / 1e3 / n_ep
+    # roofline of the dominant kernel (the fused epoch kernel) from the timed
+    # region: the epoch loop's device time per epoch
+    avg_epoch_s = max_over_ranks(np.sum(loops), dist) / args.steps / n_ep
+    dens_ms = None
+    if wl["dens"]:
+        st.set_schedule(umapcu.SCHED_SCAN)
+        st.reset(prob["init"])
+        st.set_schedule(umapcu.SCHED_BITS)
+        torch.cuda.synchronize()
+        k_ms, d_ms = st.run_profiled(0, n_ep, opt)
+        dens_ms = d_ms
+        avg_epoch_s = k_ms / 1e3 / n_ep
     n_nodes = wl["n"]
     nd = 2
-    alg_bytes = (112.0 * updates_per_step + n_ep * (8.0 * E) + 4.0 * updates_per_step
-                 + n_ep * n_nodes * nd * 4 * 7) / n_ep
+    # algorithmic HBM bytes per epoch: E (tail index + period/cursor) + A_e
+    # cursor writes + n * D * 4 B * 7 node-state streams
+    hbm_bytes = (8.0 * E * n_ep + 4.0 * updates_per_step + 28.0 * n_nodes * nd * n_ep) / n_ep
+    # algorithmic L2 gathers per epoch: 2 endpoints x (1 + neg_rate) rows of 8 B per edge-update
+    l2_bytes = 2.0 * (1 + 5) * 8.0 * updates_per_step / n_ep
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except (OSError, ValueError):
         pass
     peak = peaks.get("hbm_gbs", 6650.0)
-    achieved = alg_bytes / avg_launch_s / 1e9
+    l2_peak = umapcu.probe_l2_gather(8 * n_nodes)
     traffic = None
     tf = os.path.join(ROOT, "profiles", f"k_epoch_{args.workload}_traffic.txt")
     if os.path.exists(tf):
         for ln in open(tf):
             if ln.startswith("dram_bytes_per_launch:"):
                 traffic = float(ln.split(":")[1])
+    achieved = hbm_bytes / avg_epoch_s / 1e9
+    l2_ach = l2_bytes / avg_epoch_s / 1e9
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "traffic": traffic,
-            "kernel": "k_epoch<2,false>" if not wl["dens"] else "k_epoch<2,true>",
-            "avg_launch_us": round(avg_launch_s * 1e6, 2),
-            "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
+            "kernel": f"k_epoch<2,{'true' if wl['dens'] else 'false'},5,true,false,true> (bitmask scan)",
+            "avg_launch_us": round(avg_epoch_s * 1e6, 2),
+            "hbm_bytes_per_launch": round(hbm_bytes), "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+            "l2": {"achieved": round(l2_ach, 1), "peak": round(l2_peak, 1), "unit": "GB/s",
+                   "frac": round(l2_ach / l2_peak, 4), "bytes_per_launch": round(l2_bytes),
+                   "what": "random 8-byte coordinate gathers (2 endpoints x (1 + 5 negatives) per edge-update) "
+                           "against umapcu_probe_l2_gather's measured rate of the same gather form",
+                   "binding_unit": "L2 (ncu: lts throughput well above dram throughput)"}}
 
     # end to end through the reference-facing C-ABI call, pinned host buffers
     e2e = None
@@ -422,12 +466,11 @@ def main():
         embd_p = pin(prob["init"])
         A = umapcu.Adjacency(ptr_p, col_p, w_p)
         init = prob["init"]
-        e2e_steps = max(1, min(args.steps, 3))
-        for _ in range(1):
+        for _ in range(max(1, args.warmup)):
             embd_p[...] = init
             umapcu.optimise_embedding_adam_gpu(embd_p, A, prob["params"], prob["dens"], seed, 0, sampler, opt)
         tt = []
-        for _ in range(e2e_steps):
+        for _ in range(args.steps):
             embd_p[...] = init
             torch.cuda.synchronize()
             if dist:
@@ -437,8 +480,10 @@ def main():
             tt.append(time.perf_counter() - t0)
         et = max_over_ranks(np.sum(tt), dist)
         h2d = ptr_p.nbytes + col_p.nbytes + w_p.nbytes + embd_p.nbytes
-        e2e = {"value": world * e2e_steps * updates_per_step / et, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-               "d2h_bytes_per_step": int(embd_p.nbytes), "ms_per_step": round(et / e2e_steps * 1e3, 3)}
+        if prob["dens"] is not None:
+            h2d += prob["dens"].r.nbytes
+        e2e = {"value": world * args.steps * updates_per_step / et, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(embd_p.nbytes), "ms_per_step": round(et / args.steps * 1e3, 3)}
 
     quality = None
     if e2e is not None and rank == 0:
@@ -456,8 +501,18 @@ def main():
                          "edges; its parallel CPU path is the Adam one"}
     elif rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        v, sample, secs = cpu_windows(prob, wl, seed, args.cpu_seconds, threads)
-        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
+        adj = prob["adj"]
+        dd = None
+        if prob["dens"] is not None:
+            d = prob["dens"]
+            dd = {"r": d.r, "lambda": d.params.lambda_, "frac": d.params.frac, "var_shift": d.params.var_shift,
+                  "mu_tot": d.mu_tot}
+        secs = cpu_full_runs(adj.ptr, adj.col, adj.w, prob["params"].as_dict(), prob["init"], dd, seed, 3, threads,
+                             n_ep)
+        cpu = {"value": updates_per_step / min(secs), "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"whole {n_ep}-epoch runs of the oracle's adam_parallel restatement from the same initial "
+                         f"embedding, epoch loop only, best of 3 ({', '.join(f'{x:.2f}' for x in secs)} s; "
+                         f"{updates_per_step} edge-updates per run)"}
 
     dens_launches = 0
     if wl["dens"]:
@@ -468,23 +523,18 @@ def main():
             "metric": metric_of(wl), "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"{args.workload}: {wl['desc']}", "n_points": wl["n"], "n_edges": int(E),
-                       "edge_updates_per_step": updates_per_step, "epochs": n_ep,
-                       "sampler": args.sampler, "optimiser": args.optimiser,
-                       "schedule": ("per-epoch active-entry lists built at state creation "
-                                    f"({sched['build_ms']:.1f} ms, {sched['records']} records; outside the timed "
-                                    "region like the CSR build)") if sched["lists"] else "CSR scan every epoch",
-                       "e2e_schedule": "per-epoch active-entry bitmasks (1 bit per CSR entry and epoch), built "
-                                       "inside each timed call",
-                       "value_csr_scan": scan_value,
-                       "l2": "flushed before every step (256 MiB write)",
-                       "parallelism": f"replicas x{world}"},
+            "config": config_of(args, wl),
+            "n_edges": int(E), "edge_updates_per_step": updates_per_step, "sampler": args.sampler,
+            "schedule": "per-epoch active-entry bitmasks (1 bit per CSR entry and epoch), built inside every "
+                        "timed step, then every epoch; the graph and CSR stay resident (built once, outside)",
+            "schedule_variants": variants,
             "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": e2e,
-            "gpu_launches": args.steps * (n_ep + dens_launches),
+            # per step: the bitmask build, one fused epoch kernel per epoch, the densMAP updates
+            "gpu_launches": args.steps * (1 + n_ep + dens_launches),
             "clocks": clk.summary(),
-            "densmap_ms_per_step": round(d_ms, 3) if wl["dens"] else None,
+            "densmap_ms_per_step": round(dens_ms, 3) if dens_ms is not None else None,
             "quality": quality,
         }
         print(json.dumps(out), flush=True)
@@ -494,10 +544,20 @@ def main():
         dist.destroy_process_group()
 
 
+def init_group(world, backend="nccl"):
+    """The process group of a multi-rank run (None for one rank)."""
+    if world <= 1:
+        return None
+    import datetime
+    import torch.distributed as dist
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return dist
+
+
 def make_batch_problems(wl, seed):
     """The C4 problem set: seeded sizes, data, exact kNN, CUDA graph stage."""
     import umapcu
-    import umapcu.synth as S
+    import umapdata.synth as S
     rng = np.random.default_rng(seed)
     sizes = np.exp(rng.uniform(np.log(wl["n_lo"]), np.log(wl["n_hi"]), wl["problems"])).astype(int)
     adjs, inits = [], []
@@ -514,10 +574,12 @@ def make_batch_problems(wl, seed):
 
 
 def run_batched(args, wl, world, rank, local_rank):
-    """Batched form vs sequential single-problem runs, embeddings/s."""
+    """Batched form vs sequential single-problem runs, embeddings/s; every
+    rank runs its own problem set, times are the max over ranks."""
     import torch
     import umapcu
     torch.cuda.set_device(local_rank)
+    dist = init_group(world)
     seed = args.seed + rank
     sizes, adjs, inits = make_batch_problems(wl, seed)
     params = umapcu.UmapOptimParams.from_min_dist_spread(0.1, 1.0, n_epochs=wl["n_epochs"], neg_sample_rate=5)
@@ -528,7 +590,7 @@ def run_batched(args, wl, world, rank, local_rank):
         B.run(0)
     with ClockSampler(local_rank) as clk:
         ms = [B.run(0) for _ in range(args.steps)]
-    t_batch = float(np.sum(ms)) / 1e3
+    t_batch = max_over_ranks(float(np.sum(ms)) / 1e3, dist)
     # edge-updates per run, from each problem's periods
     updates = 0
     states = []
@@ -553,7 +615,7 @@ def run_batched(args, wl, world, rank, local_rank):
         st.run(0, wl["n_epochs"])
     e1.record(stream)
     torch.cuda.synchronize()
-    t_seq = e0.elapsed_time(e1) / 1e3
+    t_seq = max_over_ranks(e0.elapsed_time(e1) / 1e3, dist)
     # identical results in the batch and alone (spot check)
     ok = True
     for i in (0, len(sizes) // 2, len(sizes) - 1):
@@ -571,6 +633,7 @@ def run_batched(args, wl, world, rank, local_rank):
                       "autotuned": cfg, "l2": "not flushed (state reset kernel precedes every run)"},
            "edge_updates_per_s": world * args.steps * updates / t_batch,
            "sequential_plain": {"embeddings_per_s": P / t_seq, "ms": round(t_seq * 1e3, 3)},
+           "sequential_plain_total": {"embeddings_per_s": world * P / t_seq},
            "speedup_vs_sequential": round((P / t_batch * args.steps) / (P / t_seq), 2) if t_seq > 0 else None,
            "same_result_alone_and_batched": ok,
            # per run: the state reset kernel, then one persistent launch or one launch per epoch
@@ -579,14 +642,19 @@ def run_batched(args, wl, world, rank, local_rank):
     if rank == 0:
         print(json.dumps(out), flush=True)
     B.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 def run_served(args, wl, world, rank, local_rank):
-    """Continuous-batching server under a Poisson request stream."""
+    """Continuous-batching server under a Poisson request stream; every rank
+    serves its own stream, the span is the max over ranks."""
     import torch
     import umapcu
-    import umapcu.synth as S
+    import umapdata.synth as S
     torch.cuda.set_device(local_rank)
+    dist = init_group(world)
     seed = args.seed + rank
     rng = np.random.default_rng(seed)
     t0 = time.time()
@@ -648,8 +716,9 @@ def run_served(args, wl, world, rank, local_rank):
         t_end = time.perf_counter()
     st = sv.stats()
     sv.close()
-    span = t_end - t_start
-    out = {"metric": "UMAP served embeddings/s (Poisson stream)", "value": n_req / span, "unit": "embeddings/s",
+    span = max_over_ranks(t_end - t_start, dist)
+    out = {"metric": "UMAP served embeddings/s (Poisson stream)", "value": world * n_req / span,
+           "unit": "embeddings/s",
            "n_gpus": world, "steps": 1, "warmup": 0, "ms_per_step": round(span * 1e3, 3),
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
            "config": {"workload": f"c5: {wl['desc']}", "requests": n_req, "arrival_rate_per_s": round(lam, 2),
@@ -662,6 +731,9 @@ def run_served(args, wl, world, rank, local_rank):
            "server": st, "clocks": clk.summary()}
     if rank == 0:
         print(json.dumps(out), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 def run_spectral(args, wl, world, rank, local_rank):
@@ -712,31 +784,34 @@ def run_spectral(args, wl, world, rank, local_rank):
 
 
 def run_reference(args, wl, world):
-    """The reference's parallel-Adam CPU optimiser on the host cores,
-    bounded windows of the same workload (one window per step)."""
-    seed = args.seed
-    prob = make_problem(wl, seed, reference_graph=True)
+    """The reference's parallel-Adam CPU optimiser (umap_optimisers.rs:
+    1170-1492, restated in oracle/) on all host cores: every step is one
+    whole run of the workload's epochs from the initial embedding, epoch loop
+    timed. Loads no umapcu code: inputs come from umapdata and the oracle."""
+    if wl["kind"] in ("batch", "serve") or wl.get("spectral"):
+        print(json.dumps({"impl": "reference", "unavailable": f"workload {args.workload} has no counterpart in "
+                          "the reference (it optimises one embedding per call)"}), flush=True)
+        return
     from oracle import oracle as O
-    adj = prob["adj"]
-    stt, csr = O.csr_from_graph(wl["n"], adj.ptr, adj.col, adj.w)
-    prob["A_e"] = active_edges_per_epoch(csr["eps"], wl["n_epochs"])
+    seed = args.seed
+    prob = make_reference_problem(wl, seed)
+    stt, csr = O.csr_from_graph(wl["n"], prob["ptr"], prob["col"], prob["w"])
+    updates = int(active_edges_per_epoch(csr["eps"], wl["n_epochs"]).sum())
     threads = os.cpu_count() or 1
-    per_step = max(1.0, args.cpu_seconds / 2)
-    for _ in range(args.warmup):
-        cpu_windows(prob, wl, seed, per_step / 4, threads)
-    updates, samples, secs = 0.0, [], 0.0
-    for _ in range(args.steps):
-        v, s, t = cpu_windows(prob, wl, seed, per_step, threads)
-        updates += v * t
-        samples.append(s)
-        secs += t
-    value = updates / secs
+    run = lambda k: cpu_full_runs(prob["ptr"], prob["col"], prob["w"], prob["params"], prob["init"], prob["dens"],
+                                  seed, k, threads, wl["n_epochs"])
+    run(args.warmup)
+    secs = run(args.steps)
+    total = float(np.sum(secs))
+    value = args.steps * updates / total
+    sample = (f"whole {wl['n_epochs']}-epoch runs of the oracle's adam_parallel restatement from the U(-10,10) "
+              f"initial embedding, epoch loop only, one run per step ({updates} edge-updates per run, "
+              f"{min(secs):.2f}-{max(secs):.2f} s)")
     out = {"metric": metric_of(wl), "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-           "warmup": args.warmup, "ms_per_step": round(secs / args.steps * 1e3, 3), "higher_is_better": True,
+           "warmup": args.warmup, "ms_per_step": round(total / args.steps * 1e3, 3), "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
-           "config": {"workload": f"{args.workload}: {wl['desc']}", "n_points": wl["n"]},
-           "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                            "sample": samples[0]},
+           "config": config_of(args, wl),
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
 

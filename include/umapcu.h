@@ -167,6 +167,12 @@ umapcu_status umapcu_state_read_csr(const umapcu_state *st, uint32_t *offsets, u
 umapcu_status umapcu_state_run(umapcu_state *st, uint32_t first_epoch, uint32_t count,
                                uint32_t optimiser);
 
+/* umapcu_state_run without the final synchronisation: the epochs are only
+ * enqueued on the state's stream (see umapcu_state_set_stream), for callers
+ * that order their own work, or time it with events, on that stream. */
+umapcu_status umapcu_state_enqueue(umapcu_state *st, uint32_t first_epoch, uint32_t count,
+                                   uint32_t optimiser);
+
 /* One epoch with inspection hooks, for parity tests (mirrors
  * launch_grad_accum + launch_adam_update + launch_edge_schedule_update,
  * umap_optimiser_gpu.rs:1016-1227). injected: NULL or host [2E * neg_rate]
@@ -379,6 +385,45 @@ umapcu_status umapcu_sample_negatives(uint32_t sampler, uint64_t seed, uint32_t 
  * each); build_ms: list build time. */
 umapcu_status umapcu_state_schedule_info(const umapcu_state *st, int *lists_active, uint64_t *n_records,
                                          float *build_ms);
+
+/* Precomputed forms of the edge schedule a state can hold (see
+ * umapcu_state_schedule_info): none (every epoch scans and advances the
+ * cursors), per-epoch bitmasks, or per-epoch record lists. */
+enum { UMAPCU_SCHED_SCAN = 0, UMAPCU_SCHED_BITS = 1, UMAPCU_SCHED_LISTS = 2 };
+
+/* Replaces the state's precomputed schedule by `form`, built now from the
+ * edge periods on the state's stream (bitmasks: asynchronously, without a
+ * host synchronisation when nothing was held before; lists: synchronously).
+ * Results are bit-identical in every form. UMAPCU_CAPACITY when the form
+ * does not fit (half the free device memory); the state then scans. */
+umapcu_status umapcu_state_set_schedule(umapcu_state *st, uint32_t form);
+
+/* The form the state holds now (UMAPCU_SCHED_*). */
+umapcu_status umapcu_state_schedule_form(const umapcu_state *st, uint32_t *form);
+
+/* ---------------------------------------------------- memory hygiene
+ * (no counterpart in the reference, whose UmapGpuState holds device memory
+ * for one call only, umap_optimiser_gpu.rs:278-348). The library keeps two
+ * things between calls: the one-shot call's schedule-bitmask block (one per
+ * device, up to 1 bit per CSR entry and epoch) and, in each device's default
+ * stream-ordered memory pool (a process-wide object), the blocks its calls
+ * freed -- it raises that pool's release threshold, which otherwise returns
+ * freed memory to the driver at every synchronisation. */
+
+/* keep = 0: put back every pool release threshold the library raised (and
+ * trim those pools), and leave the pools alone from now on; keep = 1 (the
+ * default): raise them again on the next call. */
+umapcu_status umapcu_set_pool_retention(int keep);
+
+/* Frees the current device's cached bitmask block and trims its default
+ * pool to the memory in use. */
+umapcu_status umapcu_release_cached(void);
+
+/* Measurement hook: the rate of random 8-byte gathers from an L2-resident
+ * table of table_bytes (4 KiB .. 64 MiB), in GB/s of gathered bytes -- the
+ * load form of the epoch kernel's coordinate gathers (float2 rows,
+ * evict_last L2 policy), so the denominator of its L2 roofline. */
+umapcu_status umapcu_probe_l2_gather(uint64_t table_bytes, float *gbs);
 
 /* ------------------------------------------------ kNN, metrics, kNN cache */
 

@@ -12,6 +12,7 @@
 #include <atomic>
 #include <chrono>
 #include <memory>
+#include <mutex>
 
 #include "internal.cuh"
 #include "layout.cuh"
@@ -294,18 +295,47 @@ __global__ void k_dens_weight_out(uint32_t n, const float4 *__restrict__ dn, con
 
 // Keep freed stream-ordered allocations cached in the device's default pool
 // across calls (the default release threshold of 0 returns them to the
-// driver at every synchronisation). Process-local; set once per device.
-void umapcu::keep_pool_memory()
+// driver at every synchronisation). The pool is process-wide, so the
+// threshold the library found is remembered and put back by
+// umapcu_set_pool_retention(0), after which the library leaves it alone.
+namespace {
+std::atomic<bool> g_pool_retention{true};
+std::mutex g_pool_mu;
+struct PoolRecord {
+    bool raised = false;
+    uint64_t prev = 0;
+};
+PoolRecord g_pool[64];
+
+void restore_pool_locked(int dev)
 {
-    static std::atomic<bool> done[64] = {};
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64 || done[dev].load()) return;
+    if (!g_pool[dev].raised) return;
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
-        uint64_t thr = UINT64_MAX;
-        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+        uint64_t prev = g_pool[dev].prev;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &prev);
+        cudaMemPoolTrimTo(pool, 0);
     }
-    done[dev].store(true);
+    g_pool[dev].raised = false;
+}
+}  // namespace
+
+void umapcu::keep_pool_memory()
+{
+    if (!g_pool_retention.load()) return;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if (g_pool[dev].raised || !g_pool_retention.load()) return;
+    cudaMemPool_t pool;
+    uint64_t prev = 0, thr = UINT64_MAX;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess ||
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &prev) != cudaSuccess)
+        return;
+    if (cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr) == cudaSuccess) {
+        g_pool[dev].raised = true;
+        g_pool[dev].prev = prev;
+    }
 }
 
 // ------------------------------------------------------------------ ABI
@@ -512,6 +542,15 @@ umapcu_status umapcu_state_run(umapcu_state *st, uint32_t first_epoch, uint32_t 
         if (!st || optimiser > UMAPCU_OPT_SGD) return UMAPCU_BAD_ARG;
         for (uint32_t e = first_epoch; e < first_epoch + count; e++) run_epoch(st, e, optimiser, nullptr, nullptr, nullptr);
         sync(st->stream.s);
+        return UMAPCU_OK;
+    });
+}
+
+umapcu_status umapcu_state_enqueue(umapcu_state *st, uint32_t first_epoch, uint32_t count, uint32_t optimiser)
+{
+    return guard([&]() -> umapcu_status {
+        if (!st || optimiser > UMAPCU_OPT_SGD) return UMAPCU_BAD_ARG;
+        for (uint32_t e = first_epoch; e < first_epoch + count; e++) run_epoch(st, e, optimiser, nullptr, nullptr, nullptr);
         return UMAPCU_OK;
     });
 }
@@ -775,6 +814,73 @@ umapcu_status umapcu_sample_negatives(uint32_t sampler, uint64_t seed, uint32_t 
         launch_sample(sampler, seed, node, entry, epoch, edge_local, count, n, d.p, S.s);
         d2h(out, d.p, count, S.s);
         sync(S.s);
+        return UMAPCU_OK;
+    });
+}
+
+umapcu_status umapcu_state_set_schedule(umapcu_state *st, uint32_t form)
+{
+    return guard([&]() -> umapcu_status {
+        if (!st || form > UMAPCU_SCHED_LISTS) return UMAPCU_BAD_ARG;
+        cudaStream_t s = st->stream.s;
+        if (st->lists_ok || st->bits_ok) {
+            // cursors brought up to date, and every launch that reads the
+            // old form finished, before it is freed
+            sync_cursors(st);
+            sync(s);
+            st->lists = ScheduleLists();
+            st->bits.release();
+            st->lists_ok = st->bits_ok = false;
+        }
+        if (form == UMAPCU_SCHED_SCAN) return UMAPCU_OK;
+        if (form == UMAPCU_SCHED_LISTS) {
+            sync(s);
+            const auto t0 = std::chrono::steady_clock::now();
+            st->lists_ok = build_schedule_lists(st->csr, st->p.n_epochs, st->lists, s);
+            sync(s);
+            st->lists_build_ms =
+                (float)std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+            return st->lists_ok ? UMAPCU_OK : UMAPCU_CAPACITY;
+        }
+        st->bits_ok = build_schedule_bits(st->csr, st->p.n_epochs, st->bits, s);
+        return st->bits_ok ? UMAPCU_OK : UMAPCU_CAPACITY;
+    });
+}
+
+umapcu_status umapcu_state_schedule_form(const umapcu_state *st, uint32_t *form)
+{
+    if (!st || !form) return UMAPCU_BAD_ARG;
+    *form = st->lists_ok ? UMAPCU_SCHED_LISTS : st->bits_ok ? UMAPCU_SCHED_BITS : UMAPCU_SCHED_SCAN;
+    return UMAPCU_OK;
+}
+
+umapcu_status umapcu_set_pool_retention(int keep)
+{
+    g_pool_retention.store(keep != 0);
+    if (keep) return UMAPCU_OK;
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    for (int dev = 0; dev < 64; dev++) restore_pool_locked(dev);
+    return UMAPCU_OK;
+}
+
+umapcu_status umapcu_release_cached(void)
+{
+    return guard([&]() -> umapcu_status {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return UMAPCU_NO_DEVICE;
+        release_cached_bits();
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
+        return UMAPCU_OK;
+    });
+}
+
+umapcu_status umapcu_probe_l2_gather(uint64_t table_bytes, float *gbs)
+{
+    return guard([&]() -> umapcu_status {
+        if (!gbs || table_bytes < 4096 || table_bytes > (64ull << 20)) return UMAPCU_BAD_ARG;
+        Stream S;
+        *gbs = probe_l2_gather(table_bytes, S.s);
         return UMAPCU_OK;
     });
 }

@@ -107,7 +107,8 @@ inline unsigned ceil_div(uint64_t a, uint64_t b) { return (unsigned)((a + b - 1)
 
 int device_sm_count();
 // Keeps freed stream-ordered allocations cached in the current device's
-// default pool (release threshold raised from 0); set once per device.
+// default pool (release threshold raised from 0); set once per device, and
+// not at all after umapcu_set_pool_retention(0).
 void keep_pool_memory();
 
 // launch_adam_update host scalars (umap_optimiser_gpu.rs:1164-1175), f32:
@@ -233,8 +234,13 @@ struct ScheduleBits {
     ScheduleBits() = default;
     ScheduleBits(const ScheduleBits &) = delete;
     ScheduleBits &operator=(const ScheduleBits &) = delete;
-    ~ScheduleBits();
+    ~ScheduleBits() { release(); }
+    // Gives the block back (to the device's cache when it is empty, else to
+    // the driver) once the stream that built it is idle; `bits` then null.
+    void release();
 };
+// Frees the current device's cached bitmask block (none cached: no-op).
+void release_cached_bits();
 // Builds the bitmasks for epochs [0, n_epochs) from the reset schedule;
 // false when they would not fit (half the free device memory), `out` then
 // empty.

@@ -407,6 +407,61 @@ void launch_eval_pow(const float *x, uint32_t n, float b, bool precise, float *o
     check_launch("k_eval_pow");
 }
 
+// L2 random-gather probe: every thread issues rounds x 8 independent 8-byte
+// row gathers in the epoch kernel's load form (ld.global.nc, evict_last L2
+// policy, float2 rows) at pseudo-random rows of a table small enough to stay
+// in L2. The row of each gather comes from an integer hash chain (Wellons'
+// "lowbias32" finaliser), independent of the loaded values.
+__global__ void __launch_bounds__(256) k_l2_gather_probe(const float *__restrict__ table, uint32_t rows,
+                                                         uint32_t rounds, float *__restrict__ out)
+{
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t pol = l2_keep_policy();
+    uint32_t h = t * 0x9E3779B1u + 0x7F4A7C15u;
+    float acc = 0.0f;
+    for (uint32_t r = 0; r < rounds; r++) {
+        float v[8][2];
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            h ^= h >> 16;
+            h *= 0x7FEB352Du;
+            h ^= h >> 15;
+            h *= 0x846CA68Bu;
+            h ^= h >> 16;
+            load_row_keep<2>(table, __umulhi(h, rows), v[u], pol);
+        }
+#pragma unroll
+        for (int u = 0; u < 8; u++) acc += v[u][0] + v[u][1];
+    }
+    out[t] = acc;
+}
+
+float probe_l2_gather(uint64_t table_bytes, cudaStream_t s)
+{
+    const uint32_t rows = (uint32_t)(table_bytes / 8);
+    const uint32_t threads = 256, blocks = (uint32_t)device_sm_count() * 8, rounds = 64;
+    DevBuf<float> table((size_t)rows * 2, s), out((size_t)threads * blocks, s);
+    check_cuda(cudaMemsetAsync(table.p, 0, (size_t)rows * 8, s), "memset");
+    cudaEvent_t e0, e1;
+    check_cuda(cudaEventCreate(&e0), "cudaEventCreate");
+    check_cuda(cudaEventCreate(&e1), "cudaEventCreate");
+    float best = 1e30f;
+    for (int it = 0; it < 6; it++) {  // the first launch warms L2
+        check_cuda(cudaEventRecord(e0, s), "record");
+        k_l2_gather_probe<<<blocks, threads, 0, s>>>(table.p, rows, rounds, out.p);
+        check_launch("k_l2_gather_probe");
+        check_cuda(cudaEventRecord(e1, s), "record");
+        sync(s);
+        float ms = 0.0f;
+        check_cuda(cudaEventElapsedTime(&ms, e0, e1), "elapsed");
+        if (it > 0 && ms < best) best = ms;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    const double bytes = 8.0 * 8.0 * rounds * (double)threads * blocks;
+    return (float)(bytes / (best * 1e-3) / 1e9);
+}
+
 void launch_sample(uint32_t sampler, uint64_t seed, uint32_t node, uint32_t entry, uint32_t epoch,
                    uint32_t edge_local, uint32_t count, uint32_t n, uint32_t *out, cudaStream_t s)
 {

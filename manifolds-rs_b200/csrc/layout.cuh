@@ -66,6 +66,9 @@ void launch_adam_apply(const float *grad, const uint32_t *hu, float *m, float *v
                        uint32_t n_dim, float fused, float epsc, float omb1, float omb2, cudaStream_t s);
 void launch_schedule(const float *eps, float *cursor, uint64_t ne, uint32_t epoch, cudaStream_t s);
 void launch_eval_pow(const float *x, uint32_t n, float b, bool precise, float *out, cudaStream_t s);
+// GB/s (8 bytes per gather) of random float2 gathers from an L2-resident
+// table of table_bytes, best of five timed launches.
+float probe_l2_gather(uint64_t table_bytes, cudaStream_t s);
 void launch_sample(uint32_t sampler, uint64_t seed, uint32_t node, uint32_t entry, uint32_t epoch,
                    uint32_t edge_local, uint32_t count, uint32_t n, uint32_t *out, cudaStream_t s);
 

@@ -281,16 +281,35 @@ BitsBlock g_bits_cache[64];
 
 }  // namespace
 
-ScheduleBits::~ScheduleBits()
+void ScheduleBits::release()
 {
     if (!bits) return;
     if (built_on) cudaStreamSynchronize(built_on);
-    std::lock_guard<std::mutex> lk(g_bits_mu);
-    if (dev >= 0 && dev < 64 && !g_bits_cache[dev].p) {
-        g_bits_cache[dev] = BitsBlock{bits, cap};
-    } else {
-        cudaFree(bits);  // a concurrent call's block: the cache holds one
+    {
+        std::lock_guard<std::mutex> lk(g_bits_mu);
+        if (dev >= 0 && dev < 64 && !g_bits_cache[dev].p) {
+            g_bits_cache[dev] = BitsBlock{bits, cap};
+        } else {
+            cudaFree(bits);  // a concurrent call's block: the cache holds one
+        }
     }
+    bits = nullptr;
+    cap = 0;
+    words = 0;
+    n_epochs = 0;
+    built_on = nullptr;
+}
+
+void release_cached_bits()
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+    BitsBlock blk;
+    {
+        std::lock_guard<std::mutex> lk(g_bits_mu);
+        std::swap(blk, g_bits_cache[dev]);
+    }
+    if (blk.p) cudaFree(blk.p);
 }
 
 void launch_schedule_bits(const float2 *sched, uint64_t n_entries, uint32_t n_epochs, uint32_t *bits,

@@ -44,6 +44,7 @@ CUDA_ALLOC, CUDA_LAUNCH, TIMEOUT, BAD_ARG, NO_DEVICE, CAPACITY, CANCELLED = 4, 5
 
 OPT_ADAM, OPT_SGD = 0, 1
 NEG_REF_HASH, NEG_PHILOX = 0, 1
+SCHED_SCAN, SCHED_BITS, SCHED_LISTS = 0, 1, 2
 
 
 class ManifoldsError(RuntimeError):
@@ -152,6 +153,12 @@ _SIGS = {
     "umapcu_knn_save": [C.c_char_p, _u32, _u32, _u32, _vp, _vp],
     "umapcu_knn_load_header": [C.c_char_p, _vp, _vp, _vp],
     "umapcu_knn_load": [C.c_char_p, _u32, _u32, _vp, _vp],
+    "umapcu_state_set_schedule": [_vp, _u32],
+    "umapcu_state_enqueue": [_vp, _u32, _u32, _u32],
+    "umapcu_state_schedule_form": [_vp, _vp],
+    "umapcu_set_pool_retention": [_i32],
+    "umapcu_release_cached": [],
+    "umapcu_probe_l2_gather": [_u64, _vp],
 }
 for _name, _args in _SIGS.items():
     _fn = getattr(_lib, _name)
@@ -443,6 +450,22 @@ class UmapGpuState:
     def run(self, first_epoch: int, count: int, optimiser: int = OPT_ADAM):
         _check(_lib.umapcu_state_run(self._h, first_epoch, count, optimiser))
 
+    def enqueue(self, first_epoch: int, count: int, optimiser: int = OPT_ADAM):
+        """run() without the final synchronisation (epochs enqueued on the
+        state's stream)."""
+        _check(_lib.umapcu_state_enqueue(self._h, first_epoch, count, optimiser))
+
+    def set_schedule(self, form: int):
+        """Rebuilds the precomputed edge schedule as SCHED_SCAN (none),
+        SCHED_BITS (per-epoch bitmasks) or SCHED_LISTS (per-epoch records);
+        results are bit-identical in every form."""
+        _check(_lib.umapcu_state_set_schedule(self._h, form), "set_schedule")
+
+    def schedule_form(self) -> int:
+        f = C.c_uint32()
+        _check(_lib.umapcu_state_schedule_form(self._h, C.byref(f)))
+        return f.value
+
     def reset(self, embd=None):
         """Back to the initial state: embedding := embd, moments := 0, cursors := periods."""
         ce = None if embd is None else _c(embd, np.float32)
@@ -708,6 +731,28 @@ def sample_negatives(sampler, seed, node, entry, epoch, edge_local, count, n):
     _check(_lib.umapcu_sample_negatives(sampler, seed & (2 ** 64 - 1), node, entry, epoch, edge_local, count, n,
                                         _p(out)))
     return out
+
+
+# ------------------------------------------------------- memory hygiene
+
+def set_pool_retention(keep: bool = True):
+    """False: restore every device pool release threshold the library raised
+    and leave the pools alone from now on (see umapcu_set_pool_retention)."""
+    _check(_lib.umapcu_set_pool_retention(int(bool(keep))))
+
+
+def release_cached():
+    """Frees the current device's cached schedule-bitmask block and trims its
+    default memory pool."""
+    _check(_lib.umapcu_release_cached(), "release_cached")
+
+
+def probe_l2_gather(table_bytes: int = 8 << 20) -> float:
+    """GB/s of random 8-byte gathers from an L2-resident table (the epoch
+    kernel's coordinate-gather form): the L2 roofline denominator."""
+    g = C.c_float()
+    _check(_lib.umapcu_probe_l2_gather(int(table_bytes), C.byref(g)), "probe_l2_gather")
+    return g.value
 
 
 # ------------------------------------------------------- kNN and metrics

@@ -68,6 +68,13 @@ def subspace_mixture(n, dim, n_clusters, seed, sub_dim=3, mean_sd=6.0, sd=1.0, n
     return X.astype(np.float32), lab.astype(np.int32)
 
 
+def random_layout(n_samples, n_comp, seed, init_range=10.0):
+    """U(-range, range) initial embedding from numpy's PCG64 stream seeded
+    with `seed` (the values umapcu.random_layout returns)."""
+    rng = np.random.default_rng(seed)
+    return rng.uniform(-init_range, init_range, (n_samples, n_comp)).astype(np.float32)
+
+
 def _finish(i_idx, d2, k):
     """Drop self (or the farthest if self is absent), sort ascending."""
     n = i_idx.shape[0]

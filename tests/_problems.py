@@ -8,7 +8,7 @@ from oracle import oracle as O
 
 @functools.lru_cache(maxsize=8)
 def knn_problem(n=3000, dim=50, k=15, clusters=10, seed=0, kind="isotropic"):
-    import umapcu.synth as S
+    import umapdata.synth as S
     if kind == "subspace":
         X, lab = S.subspace_mixture(n, dim, clusters, seed)
     else:
@@ -31,7 +31,7 @@ def init_embedding(n, d=2, seed=7):
 
 def knn_preservation(X_idx, Y, k=15):
     """mean |kNN_X(i) & kNN_Y(i)| / k over all points (exact, small n)."""
-    import umapcu.synth as S
+    import umapdata.synth as S
     yi, _ = S.exact_knn_cpu(Y, k)
     return float(np.mean([len(set(a[:k]) & set(b)) / k for a, b in zip(X_idx, yi)]))
 

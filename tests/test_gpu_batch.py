@@ -10,7 +10,7 @@ umapcu = pytest.importorskip("umapcu")
 
 @pytest.fixture(scope="module")
 def problems():
-    import umapcu.synth as S
+    import umapdata.synth as S
     rng = np.random.default_rng(0)
     sizes = [300, 4700, 800, 33, 2500, 1200, 5000, 64, 900, 3100, 1500, 2000]
     out = []

@@ -17,7 +17,7 @@ umapcu = pytest.importorskip("umapcu")
 
 @pytest.fixture(scope="module")
 def dens_problem():
-    import umapcu.synth as S
+    import umapdata.synth as S
     X, lab = S.variable_density_mixture(3000, 30, 8, seed=4)
     idx, dist = S.exact_knn_cpu(X, 30)
     (r, c, v), _, _ = O.construct_umap_graph(idx, dist, 200)

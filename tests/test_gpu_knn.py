@@ -13,7 +13,7 @@ from tests._problems import fuzzy_cross_entropy, oracle_graph
 
 
 def _data(n, dim, seed, clustered=True):
-    import umapcu.synth as S
+    import umapdata.synth as S
     if clustered:
         X, _ = S.isotropic_mixture(n, dim, 6, seed)
         return np.ascontiguousarray(X, np.float32)

@@ -84,7 +84,7 @@ def test_lists_equal_scan_densmap():
 
 
 def test_lists_equal_scan_warp_per_segment():
-    import umapcu.synth as S
+    import umapdata.synth as S
     n = 60000  # 1875 segments: above the block-per-segment threshold
     X, _ = S.isotropic_mixture(n, 20, 10, 3)
     idx, dist = umapcu.knn_exact(X, 15)
@@ -149,7 +149,7 @@ def test_one_shot_bitmask_equals_scan_densmap_3d():
 
 
 def test_one_shot_bitmask_warp_per_segment_equals_scan():
-    import umapcu.synth as S
+    import umapdata.synth as S
     n = 60000  # above the block-per-segment threshold: the warp-per-segment bitmask scan
     X, _ = S.isotropic_mixture(n, 20, 10, 4)
     idx, dist = umapcu.knn_exact(X, 15)
@@ -201,3 +201,47 @@ def test_one_shot_concurrent_calls_share_the_bitmask_cache(prob):
             t.join()
         for i in range(4):
             assert np.array_equal(outs[i], alone[i]), i
+
+
+def test_set_schedule_forms_and_enqueue_are_bit_identical(prob):
+    """umapcu_state_set_schedule rebuilds the precomputed schedule in each
+    form mid-life (the bench builds the bitmasks inside every timed step);
+    enqueue() is run() without the final synchronisation. All forms and
+    both calls give identical results."""
+    import torch
+    g, adj = prob
+    p = umapcu.UmapOptimParams(n_epochs=80)
+    emb = init_embedding(3000, 2, seed=12)
+    st = _state(adj, emb, p, True)
+    assert st.schedule_form() == umapcu.SCHED_LISTS
+    ref = None
+    stream = torch.cuda.current_stream()
+    for form in (umapcu.SCHED_SCAN, umapcu.SCHED_BITS, umapcu.SCHED_LISTS, umapcu.SCHED_BITS):
+        st.set_schedule(umapcu.SCHED_SCAN)
+        st.reset(emb)
+        st.set_schedule(form)
+        assert st.schedule_form() == form
+        st.set_stream(stream.cuda_stream)
+        st.enqueue(0, 30)
+        st.run(30, 50)
+        y = st.read()[0]
+        ref = y if ref is None else ref
+        assert np.array_equal(y, ref), form
+    st.close()
+
+
+def test_release_cached_and_pool_retention():
+    """The memory-hygiene entry points run on a device with the caches in
+    use and leave the library working."""
+    g = oracle_graph(n=3000, dim=50, k=15, n_epochs=80)
+    adj = umapcu.Adjacency(g["ptr"], g["col"], g["val"])
+    p = umapcu.UmapOptimParams(n_epochs=40)
+    e1 = init_embedding(3000, 2, seed=1)
+    e2 = e1.copy()
+    umapcu.optimise_embedding_adam_gpu(e1, adj, p, seed=5)
+    umapcu.release_cached()
+    umapcu.set_pool_retention(False)
+    umapcu.optimise_embedding_adam_gpu(e2, adj, p, seed=5)
+    umapcu.set_pool_retention(True)
+    assert np.array_equal(e1, e2)
+    assert umapcu.probe_l2_gather(8 << 20) > 100.0

@@ -16,7 +16,7 @@ umapcu = pytest.importorskip("umapcu")
 
 @pytest.fixture(scope="module")
 def pool():
-    import umapcu.synth as S
+    import umapdata.synth as S
     out = []
     for i, n in enumerate([400, 2600, 1100, 5200, 700, 3300, 1800, 90]):
         X, _ = S.isotropic_mixture(n, 20, 3 + i % 5, seed=300 + i)

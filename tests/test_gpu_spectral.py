@@ -87,7 +87,7 @@ def _strip_graph(n, seed=0):
     """kNN fuzzy graph of points uniform on a 3 x 1 strip: the two lowest
     non-trivial modes of -D^-1/2 A D^-1/2 run along the long side and are
     separated from the next by a wide gap (a well-defined 2-D subspace)."""
-    import umapcu.synth as S
+    import umapdata.synth as S
     from oracle import oracle as O
     X = np.random.default_rng(seed).uniform([0.0, 0.0], [3.0, 1.0], (n, 2)).astype(np.float32)
     idx, dist = S.exact_knn_cpu(X, 15)

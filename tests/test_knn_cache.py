@@ -95,3 +95,47 @@ def test_oracle_trustworthiness_matches_sklearn(seed):
     # near tie may swap, moving one rank by one; allow ten such swaps
     unit = 2.0 / (500 * 15 * (2.0 * 500 - 3 * 15 - 1))
     assert abs(O.trustworthiness(X, Y, 15) - trustworthiness(X, Y, n_neighbors=15)) <= 10 * unit
+
+
+def test_numpy_reader_and_writer_match_the_library(tmp_path):
+    """umapdata.knn_cache (NumPy, no CUDA library) reads what umapcu_knn_save
+    writes and writes what umapcu_knn_load reads, byte for byte."""
+    from umapdata import knn_cache
+    i, d = _knn(n=257, k=7, seed=3)
+    a, b = str(tmp_path / "lib.knn"), str(tmp_path / "np.knn")
+    umapcu.save_knn(a, i, d)
+    knn_cache.save(b, i, d)
+    assert open(a, "rb").read() == open(b, "rb").read()
+    i2, d2, m = knn_cache.load(a)
+    assert np.array_equal(i, i2) and np.array_equal(d, d2) and m == knn_cache.METRIC_EUCLIDEAN_SQ
+    i3, d3, _ = umapcu.load_knn(b)
+    assert np.array_equal(i, i3) and np.array_equal(d, d3)
+    assert knn_cache.header(b) == (257, 7, 0)
+
+
+@pytest.mark.parametrize("corrupt", ["payload_bit", "truncate", "extra", "magic", "index_range"])
+def test_numpy_reader_rejects_damaged_files(tmp_path, corrupt):
+    from umapdata import knn_cache
+    i, d = _knn()
+    if corrupt == "index_range":
+        i = i.copy()
+        i[3, 2] = 300
+    p = str(tmp_path / "c.knn")
+    knn_cache.save(p, i, d)
+    b = bytearray(open(p, "rb").read())
+    if corrupt == "payload_bit":
+        b[48 + 4 * 17] ^= 0x10
+    elif corrupt == "truncate":
+        b = b[:-4]
+    elif corrupt == "extra":
+        b += b"\0"
+    elif corrupt == "magic":
+        b[0] = ord("X")
+    open(p, "wb").write(bytes(b))
+    with pytest.raises(ValueError):
+        knn_cache.load(p)
+
+
+def test_random_layout_streams_agree():
+    import umapdata.synth as S
+    assert np.array_equal(S.random_layout(1000, 2, 17), umapcu.random_layout(1000, 2, 17))

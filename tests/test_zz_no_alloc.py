@@ -23,7 +23,7 @@ umapcu = pytest.importorskip("umapcu")
 
 
 def _problem():
-    import umapcu.synth as S
+    import umapdata.synth as S
     X, _ = S.isotropic_mixture(2500, 20, 6, seed=3)
     idx, dist = S.exact_knn_cpu(X, 15)
     g = umapcu.construct_umap_graph(idx, dist, umapcu.UmapGraphParams(), 60)
