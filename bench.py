@@ -517,7 +517,7 @@ def main():
     dens_launches = 0
     if wl["dens"]:
         dp = prob["dens"]
-        dens_launches = 4 * sum(1 for e in range(n_ep) if dp.is_active(e, n_ep))
+        dens_launches = sum(1 for e in range(n_ep) if dp.is_active(e, n_ep))
     if rank == 0:
         out = {
             "metric": metric_of(wl), "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,

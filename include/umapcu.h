@@ -280,6 +280,12 @@ typedef struct umapcu_server umapcu_server;
 umapcu_status umapcu_server_create(uint64_t device_budget_bytes, uint32_t max_jobs, uint32_t tick_epochs,
                                    uint32_t n_dim, umapcu_server **out);
 
+/* The device-memory estimate the server's admission charges a job against
+ * its budget (the CSR build's temporaries dominate): for placement front
+ * ends that spread jobs over several servers. */
+umapcu_status umapcu_server_job_bytes(uint32_t n, uint32_t n_dim, uint64_t nnz, uint32_t n_epochs,
+                                      uint64_t *bytes);
+
 /* Queues one job (the arguments of umapcu_optimise_embedding, copied) and
  * returns at once with its ticket. UMAPCU_CAPACITY if the job alone exceeds
  * the budget. */
@@ -418,6 +424,12 @@ umapcu_status umapcu_set_pool_retention(int keep);
 /* Frees the current device's cached bitmask block and trims its default
  * pool to the memory in use. */
 umapcu_status umapcu_release_cached(void);
+
+/* Devices (no counterpart in the reference, which takes one device per
+ * call). Every entry point works on the calling thread's current CUDA
+ * device; a multi-device front end selects it per call. */
+umapcu_status umapcu_device_count(int *count);
+umapcu_status umapcu_set_device(int device);
 
 /* Measurement hook: the rate of random 8-byte gathers from an L2-resident
  * table of table_bytes (4 KiB .. 64 MiB), in GB/s of gathered bytes -- the

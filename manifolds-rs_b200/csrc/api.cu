@@ -39,8 +39,8 @@ struct umapcu_state {
     float lambda = 0, frac = 0, var_shift = 0, mu_tot = 0;
     DevBuf<float> r;
     DevBuf<float4> dens_node;
-    DevBuf<double> part1, mean;
-    DevBuf<double2> part2;
+    DevBuf<double> part;
+    DevBuf<uint32_t> ticket;
     DevBuf<float> stats;
     // schedule lists (schedule.cu): usable while the epochs run so far are
     // 0, 1, ..., sched_epoch - 1 from the reset schedule; the cursors in
@@ -94,9 +94,8 @@ void dens_update(umapcu_state *st)
     D.b = st->p.b;
     D.r = st->r.p;
     D.dens_node = st->dens_node.p;
-    D.part1 = st->part1.p;
-    D.part2 = st->part2.p;
-    D.mean = st->mean.p;
+    D.part = st->part.p;
+    D.ticket = st->ticket.p;
     D.stats = st->stats.p;
     D.var_shift = st->var_shift;
     D.lambda = st->lambda;
@@ -258,9 +257,9 @@ umapcu_status create_state(const float *embd, uint32_t n, uint32_t n_dim, const 
         st->dens_node.alloc(n, s);
         check_cuda(cudaMemsetAsync(st->dens_node.p, 0, n * sizeof(float4), s), "memset dens");
         const uint32_t np = dens_partials(n);
-        st->part1.alloc(np, s);
-        st->part2.alloc(np, s);
-        st->mean.alloc(1, s);
+        st->part.alloc(4ull * np, s);
+        st->ticket.alloc(1, s);
+        check_cuda(cudaMemsetAsync(st->ticket.p, 0, sizeof(uint32_t), s), "memset ticket");
         st->stats.alloc(8, s);
         check_cuda(cudaMemsetAsync(st->stats.p, 0, 8 * sizeof(float), s), "memset stats");
     }
@@ -873,6 +872,30 @@ umapcu_status umapcu_release_cached(void)
         if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
         return UMAPCU_OK;
     });
+}
+
+umapcu_status umapcu_device_count(int *count)
+{
+    if (!count) return UMAPCU_BAD_ARG;
+    *count = 0;
+    int c = 0;
+    if (cudaGetDeviceCount(&c) != cudaSuccess) {
+        cudaGetLastError();
+        return UMAPCU_NO_DEVICE;
+    }
+    *count = c;
+    return UMAPCU_OK;
+}
+
+umapcu_status umapcu_set_device(int device)
+{
+    int c = 0;
+    if (cudaGetDeviceCount(&c) != cudaSuccess) {
+        cudaGetLastError();
+        return UMAPCU_NO_DEVICE;
+    }
+    if (device < 0 || device >= c) return UMAPCU_BAD_ARG;
+    return cudaSetDevice(device) == cudaSuccess ? UMAPCU_OK : UMAPCU_NO_DEVICE;
 }
 
 umapcu_status umapcu_probe_l2_gather(uint64_t table_bytes, float *gbs)

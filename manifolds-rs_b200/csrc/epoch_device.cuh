@@ -193,12 +193,17 @@ __device__ __forceinline__ float dens_weight(float r, float re, const float *__r
     return r - st[2] * (re - st[0]) * st[3];
 }
 
-template <int D, int KU = kU>
+// Per-warp shared memory of the segment walk. The queue holds the CSR
+// positions (and, for the cursor scan, the other endpoints) of active
+// entries not yet evaluated: one super-chunk plus the carried partial batch
+// for the cursor scan; for the bitmask scan, a group of 32 bit words (1024
+// entries) plus the carried partial batch.
+template <int D, int KU = kU, bool BITS = false>
 struct WarpSmem {
-    static constexpr int kQ = 32 * KU + 32;
+    static constexpr int kQ = BITS ? 32 * 32 + 32 : 32 * KU + 32;
     uint32_t beg[33];
     uint32_t qp[kQ];
-    uint32_t qo[kQ];
+    uint32_t qo[BITS ? 1 : kQ];
     float ys[32][D];
     float part[32][D];
     float4 dn[32];
@@ -224,8 +229,8 @@ __device__ __forceinline__ uint32_t local_node(const uint32_t *beg, uint32_t p)
 // removes the per-negative and per-term uniform branches of the general path.
 // The batch's per-node sums go to part[j] for the nodes in the returned
 // mask; unless SPLIT, the node's lane then adds them to g (and sets act).
-template <int D, bool DENS, int NR, bool COH, int KU, bool FAST, bool SPLIT = false>
-__device__ __forceinline__ unsigned process_batch(const EpochArgs &A, WarpSmem<D, KU> &S, bool live, uint32_t p,
+template <int D, bool DENS, int NR, bool COH, int KU, bool FAST, bool SPLIT = false, class Smem = WarpSmem<D, KU>>
+__device__ __forceinline__ unsigned process_batch(const EpochArgs &A, Smem &S, bool live, uint32_t p,
                                                   uint32_t o, uint32_t j, uint32_t edge_local, uint32_t node0,
                                                   int lane, float (&g)[D], bool &act, const float *dstat,
                                                   float (*part)[D])
@@ -369,9 +374,8 @@ __device__ __forceinline__ unsigned process_batch(const EpochArgs &A, WarpSmem<D
 
 // The segment's row starts, positions (and densMAP node data) into shared
 // memory; ys = the lane's node's position (zeros beyond n).
-template <int D, bool DENS, bool COH, int KU>
-__device__ __forceinline__ void load_segment(const EpochArgs &A, WarpSmem<D, KU> &S, uint32_t node0, int lane,
-                                             float (&ys)[D])
+template <int D, bool DENS, bool COH, class Smem>
+__device__ __forceinline__ void load_segment(const EpochArgs &A, Smem &S, uint32_t node0, int lane, float (&ys)[D])
 {
     const uint32_t node = node0 + lane;
     const bool valid = node < A.n;
@@ -426,7 +430,7 @@ __device__ __forceinline__ void finish_node(const EpochArgs &A, uint32_t node, c
 // the entries' (cursor, period) and writes no cursor.
 template <int D, bool DENS, int NR, bool COH, int KU = kU, bool FAST = false, bool LIST = false,
           bool BITS = false>
-__device__ __forceinline__ void epoch_segment(const EpochArgs &A, WarpSmem<D, KU> &S, uint32_t node0, int lane)
+__device__ __forceinline__ void epoch_segment(const EpochArgs &A, WarpSmem<D, KU, BITS> &S, uint32_t node0, int lane)
 {
     __syncwarp();  // the warp's shared memory may still be read by its previous segment
     const uint32_t node = node0 + lane;
@@ -455,6 +459,70 @@ __device__ __forceinline__ void epoch_segment(const EpochArgs &A, WarpSmem<D, KU
             if (q + 32 + lane < r1) nx = __ldcs(A.rec + q + 32 + lane);
             process_batch<D, DENS, NR, COH, KU, FAST>(A, S, live, p, o, j, el, node0, lane, g, act, dstat, S.part);
         }
+    } else if constexpr (BITS) {
+        // The epoch's bit words, a lane per word (32 CSR entries), 32 words at
+        // a time: the words are masked to the segment, an exclusive warp
+        // prefix of their popcounts gives each lane its first queue slot, and
+        // each lane writes the positions of its set bits in ascending order --
+        // so the queue holds the active entries in CSR order, and every 32 of
+        // them form a batch exactly as in the cursor scan below. The other
+        // endpoint is loaded for active entries only, one batch ahead.
+        const uint32_t seg_beg = S.beg[0], seg_end = S.beg[32];
+        uint32_t count = 0;
+        for (uint32_t g0 = seg_beg >> 5; (uint64_t)g0 * 32u < seg_end; g0 += 32u) {
+            const uint64_t wb = (uint64_t)(g0 + lane) * 32u;
+            uint32_t m = 0;
+            if (wb < seg_end) {
+                m = __ldg(A.bits + g0 + lane);
+                if (wb < seg_beg) m &= ~0u << (seg_beg - (uint32_t)wb);
+                if (seg_end - wb < 32u) m &= (1u << (uint32_t)(seg_end - wb)) - 1u;
+            }
+            const uint32_t c = __popc(m);
+            uint32_t x = c;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const uint32_t y = __shfl_up_sync(kFull, x, off);
+                if (lane >= off) x += y;
+            }
+            uint32_t slot = count + x - c;
+            while (m) {
+                S.qp[slot++] = (uint32_t)wb + (uint32_t)(__ffs(m) - 1);
+                m &= m - 1u;
+            }
+            count += __shfl_sync(kFull, x, 31);
+            __syncwarp();
+            const bool last = (uint64_t)(g0 + 32u) * 32u >= seg_end;
+            const uint32_t upto = last ? count : (count & ~31u);
+            uint32_t p = 0, o = 0;
+            if ((uint32_t)lane < upto) {
+                p = S.qp[lane];
+                o = __ldcs(A.other + p);
+            }
+            for (uint32_t q0 = 0; q0 < upto; q0 += 32) {
+                const bool live = q0 + lane < upto;
+                uint32_t pn = 0, on = 0;
+                if (q0 + 32u + lane < upto) {
+                    pn = S.qp[q0 + 32u + lane];
+                    on = __ldcs(A.other + pn);
+                }
+                uint32_t j = 0, el = 0;
+                if (live) {
+                    j = local_node(S.beg, p);
+                    el = p - S.beg[j];
+                }
+                process_batch<D, DENS, NR, COH, KU, FAST>(A, S, live, p, o, j, el, node0, lane, g, act, dstat, S.part);
+                p = pn;
+                o = on;
+            }
+            const uint32_t rem = count - upto;
+            if (upto && rem) {
+                const uint32_t tp = (uint32_t)lane < rem ? S.qp[upto + lane] : 0u;
+                __syncwarp();
+                if ((uint32_t)lane < rem) S.qp[lane] = tp;
+            }
+            __syncwarp();
+            count = rem;
+        }
     } else {
     const uint32_t seg_beg = S.beg[0], seg_end = S.beg[32];
     const unsigned lt_mask = (1u << lane) - 1u;
@@ -464,29 +532,22 @@ __device__ __forceinline__ void epoch_segment(const EpochArgs &A, WarpSmem<D, KU
     // issued before the first is used.
     for (uint32_t c0 = seg_beg; c0 < seg_end; c0 += 32u * KU) {
         float2 sv[KU];
-        uint32_t ov[KU], bw[KU];
+        uint32_t ov[KU];
 #pragma unroll
         for (int u = 0; u < KU; u++) {
             const uint32_t p = c0 + 32u * u + lane;
             sv[u] = make_float2(__int_as_float(0x7f800000), 0.0f);
             ov[u] = 0;
-            bw[u] = 0;
             if (p < seg_end) {
-                if constexpr (BITS) bw[u] = __ldg(A.bits + (p >> 5));
-                else sv[u] = COH ? __ldcg(A.sched + p) : __ldcs(A.sched + p);
+                sv[u] = COH ? __ldcg(A.sched + p) : __ldcs(A.sched + p);
                 ov[u] = __ldcs(A.other + p);
             }
         }
 #pragma unroll
         for (int u = 0; u < KU; u++) {
             const uint32_t p = c0 + 32u * u + lane;
-            bool a;
-            if constexpr (BITS) {
-                a = (bw[u] >> (p & 31u)) & 1u;  // out-of-range lanes hold 0
-            } else {
-                a = sv[u].x <= A.epoch_f;  // out-of-range lanes hold +inf
-                if (a) __stcs(cursor + 2 * (uint64_t)p, sv[u].x + sv[u].y);  // umap_edge_schedule_update
-            }
+            const bool a = sv[u].x <= A.epoch_f;  // out-of-range lanes hold +inf
+            if (a) __stcs(cursor + 2 * (uint64_t)p, sv[u].x + sv[u].y);  // umap_edge_schedule_update
             const unsigned mask = __ballot_sync(kFull, a);
             if (a) {
                 const uint32_t slot = count + __popc(mask & lt_mask);
@@ -612,7 +673,8 @@ constexpr uint32_t kSplitWords = 256;
 // bit. Partials are added in batch order as in epoch_segment_split, so the
 // result is bit-identical to the scan.
 template <int D, bool DENS, int NR, bool FAST>
-__device__ __forceinline__ void epoch_segment_split_bits(const EpochArgs &A, WarpSmem<D, kU> &S, float (*part)[32][D],
+__device__ __forceinline__ void epoch_segment_split_bits(const EpochArgs &A, WarpSmem<D, kU, true> &S,
+                                                         float (*part)[32][D],
                                                          unsigned *has_w, uint32_t *wm, uint32_t *pre,
                                                          uint32_t node0, int warp, int lane)
 {

@@ -5,10 +5,10 @@
 //   umap_adam_update     :887-923   > fused into k_epoch
 //   umap_edge_schedule_update :940-955 /
 //   gpu_hash_neg         :611-624  -> sample_neg (bit-exact), or Philox4x32-10
-//   umap_dens_radii      :487-544  -> k_dens_radii (+ f64 partial sums)
-//   umap_dens_weights    :568-586  + host correlation_stats (density.rs:464-508)
-//                                  -> k_dens_mean / k_dens_moments / k_dens_final on the
-//                                     device; the weight is evaluated inside k_epoch
+//   umap_dens_radii      :487-544  \
+//   umap_dens_weights    :568-586   > k_dens_update, one launch (radii, f64 statistics in
+//   correlation_stats (density.rs:464-508) /  its last block); the weight is evaluated
+//                                     inside k_epoch
 //
 // k_epoch: one warp owns a segment of 32 consecutive nodes and walks the CSR
 // entries of those nodes (edges sorted by head vertex) in chunks of 32. Each
@@ -47,7 +47,7 @@ template <int D, bool DENS, int NR, bool FAST = false, bool LIST = false, bool B
 __global__ void __launch_bounds__(kWarps * 32, 6) k_epoch(const EpochArgs A)
 {
     constexpr int KU = LIST ? 1 : kU;  // the list path keeps no scan queue
-    __shared__ WarpSmem<D, KU> smem[kWarps];
+    __shared__ WarpSmem<D, KU, BITS> smem[kWarps];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t node0 = (blockIdx.x * kWarps + warp) * 32u;
     if (node0 >= A.n) return;
@@ -71,7 +71,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_epoch_split(const EpochArgs A)
 template <int D, bool DENS, int NR, bool FAST>
 __global__ void __launch_bounds__(kWarps * 32) k_epoch_split_bits(const EpochArgs A)
 {
-    __shared__ WarpSmem<D, kU> seg;
+    __shared__ WarpSmem<D, kU, true> seg;
     __shared__ float part[kWarps][32][D];
     __shared__ unsigned has_w[kWarps];
     __shared__ uint32_t wm[kSplitWords], pre[kSplitWords + 1];
@@ -82,21 +82,35 @@ __global__ void __launch_bounds__(kWarps * 32) k_epoch_split_bits(const EpochArg
 // ------------------------------------------------------------ densMAP
 
 constexpr int kDensBlock = 256;
+// Entries of a segment are taken in super-chunks of kDensU x 32: all their
+// `other` loads, then all their coordinate gathers, are issued before any is
+// used.
+constexpr int kDensU = 4;
 
-// umap_dens_radii (umap_optimiser_gpu.rs:503-543): per node, over its CSR
-// entries, sum phi and phi * d^2, then re = log(1e-8 + sum_sq / sum_phi).
-// Warp per 32-node segment (the block's 8 warps cover its 256 nodes): lanes
-// take consecutive CSR entries of the segment (coalesced `other` loads,
-// independent embedding gathers), and per-node sums come from a segmented
-// warp scan keyed by the entry's node, added to the node's lane. A
-// fixed-order f64 partial sum of the log radii per block follows.
+struct DensSums {
+    double s_re, s_re2, s_rer, s_r;
+};
+
+// One densMAP update in one launch: umap_dens_radii (umap_optimiser_gpu.rs:
+// 503-543) per node -- over all its CSR entries, phi = 1 / (1 + a d^2b),
+// sums of phi and phi * d^2, re = log(1e-8 + sum_sq / max(sum_phi, eps)) --
+// then correlation_stats (density.rs:464-508) and the weight scalars of
+// launch_dens_update (umap_optimiser_gpu.rs:1123-1142) for the whole
+// embedding.
+// Radii: a warp per 32-node segment (the block's 8 warps cover its 256
+// nodes); lanes take consecutive CSR entries of the segment, and per-node
+// sums come from a segmented warp scan keyed by the entry's node, added to
+// the node's lane chunk by chunk.
+// Statistics: each block writes f64 sums of re, re^2, re * r and r over its
+// nodes (a fixed warp-tree order); the last block to finish (atomic ticket
+// after a fence) adds the blocks' sums in a fixed order and forms
+// mean = S_re / n, var = (S_re2 - S_re^2 / n) / (n - 1),
+// cov = (S_rer - mean * S_r) / (n - 1) -- the reference's two-pass f64
+// moments in one pass, equal to them to f64 rounding -- then writes
+// stats = {mean, std, cov, 1 / std^2, lambda * mu_tot / (std * (n - 1))} in
+// f32 and re-arms the ticket for the next launch.
 template <int D>
-__global__ void __launch_bounds__(kDensBlock) k_dens_radii(uint32_t n, const uint32_t *__restrict__ offsets,
-                                                            const uint32_t *__restrict__ other,
-                                                            const float *__restrict__ y, float a, float b,
-                                                            bool precise, const float *__restrict__ r,
-                                                            float4 *__restrict__ dens_node,
-                                                            double *__restrict__ part)
+__global__ void __launch_bounds__(kDensBlock) k_dens_update(const DensArgs A)
 {
     constexpr int kW = kDensBlock / 32;
     struct Seg {
@@ -105,17 +119,20 @@ __global__ void __launch_bounds__(kDensBlock) k_dens_radii(uint32_t n, const uin
         float sums[32][2];
     };
     __shared__ Seg sm[kW];
-    __shared__ double shw[kW];
+    __shared__ DensSums shw[kW];
+    __shared__ DensSums red[kDensBlock];
+    __shared__ bool is_last;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t n = A.n;
     Seg &S = sm[warp];
     const uint32_t node0 = blockIdx.x * kDensBlock + warp * 32u;
     const uint32_t node = node0 + lane;
     const bool valid = node < n;
     const uint32_t nc = min(node0, n);
-    S.beg[lane] = offsets[valid ? node : n];
-    if (lane == 31) S.beg[32] = offsets[min(nc + 32u, n)];
+    S.beg[lane] = A.offsets[valid ? node : n];
+    if (lane == 31) S.beg[32] = A.offsets[min(nc + 32u, n)];
     float ys[D];
-    if (valid) load_row<D>(y, node, ys);
+    if (valid) load_row<D>(A.y, node, ys);
     else {
 #pragma unroll
         for (int d = 0; d < D; d++) ys[d] = 0.0f;
@@ -124,146 +141,144 @@ __global__ void __launch_bounds__(kDensBlock) k_dens_radii(uint32_t n, const uin
     for (int d = 0; d < D; d++) S.ys[lane][d] = ys[d];
     __syncwarp();
     const uint32_t seg_beg = S.beg[0], seg_end = S.beg[32];
+    const uint64_t pol = l2_keep_policy();
     float sum_sq = 0.0f, sum_phi = 0.0f;
-    for (uint32_t c0 = seg_beg; c0 < seg_end; c0 += 32u) {
-        const uint32_t p = c0 + lane;
-        const bool live = p < seg_end;
-        uint32_t j = 32;
-        float t[2] = {0.0f, 0.0f};
-        if (live) {
-            j = local_node(S.beg, p);
-            float yo[D];
-            load_row<D>(y, other[p], yo);
-            float dist_sq = 0.0f;
+    for (uint32_t c0 = seg_beg; c0 < seg_end; c0 += 32u * kDensU) {
+        uint32_t o[kDensU];
+        float yo[kDensU][D];
 #pragma unroll
-            for (int d = 0; d < D; d++) {
-                float diff = S.ys[j][d] - yo[d];
-                dist_sq += diff * diff;
+        for (int u = 0; u < kDensU; u++) {
+            const uint32_t p = c0 + 32u * u + lane;
+            o[u] = p < seg_end ? __ldcs(A.other + p) : 0u;
+        }
+#pragma unroll
+        for (int u = 0; u < kDensU; u++) {
+            const uint32_t p = c0 + 32u * u + lane;
+            if (p < seg_end) load_row_keep<D>(A.y, o[u], yo[u], pol);
+        }
+#pragma unroll
+        for (int u = 0; u < kDensU; u++) {
+            if (c0 + 32u * u >= seg_end) break;  // warp-uniform
+            const uint32_t p = c0 + 32u * u + lane;
+            const bool live = p < seg_end;
+            uint32_t j = 32;
+            float t[2] = {0.0f, 0.0f};
+            if (live) {
+                j = local_node(S.beg, p);
+                float dist_sq = 0.0f;
+#pragma unroll
+                for (int d = 0; d < D; d++) {
+                    float diff = S.ys[j][d] - yo[u][d];
+                    dist_sq += diff * diff;
+                }
+                float dist_sq_b = pow_pos(dist_sq, A.b, A.precise_pow);
+                float phi = 1.0f / (1.0f + A.a * dist_sq_b);
+                t[0] = phi * dist_sq;
+                t[1] = phi;
             }
-            float dist_sq_b = pow_pos(dist_sq, b, precise);
-            float phi = 1.0f / (1.0f + a * dist_sq_b);
-            t[0] = phi * dist_sq;
-            t[1] = phi;
-        }
-        const uint32_t jprev = __shfl_up_sync(kFull, j, 1);
-        const uint32_t jnext = __shfl_down_sync(kFull, j, 1);
-        const unsigned heads = __ballot_sync(kFull, lane == 0 || jprev != j);
-        const int start = 31 - __clz(heads & (lane == 31 ? kFull : ((2u << lane) - 1u)));
+            const uint32_t jprev = __shfl_up_sync(kFull, j, 1);
+            const uint32_t jnext = __shfl_down_sync(kFull, j, 1);
+            const unsigned heads = __ballot_sync(kFull, lane == 0 || jprev != j);
+            const int start = 31 - __clz(heads & (lane == 31 ? kFull : ((2u << lane) - 1u)));
 #pragma unroll
-        for (int off = 1; off < 32; off <<= 1) {
+            for (int off = 1; off < 32; off <<= 1) {
 #pragma unroll
-            for (int q = 0; q < 2; q++) {
-                const float v = __shfl_up_sync(kFull, t[q], off);
-                if (lane - off >= start) t[q] += v;
+                for (int q = 0; q < 2; q++) {
+                    const float v = __shfl_up_sync(kFull, t[q], off);
+                    if (lane - off >= start) t[q] += v;
+                }
             }
+            const bool tail = live && (lane == 31 || jnext != j);
+            if (tail) {
+                S.sums[j][0] = t[0];
+                S.sums[j][1] = t[1];
+            }
+            const unsigned has = __reduce_or_sync(kFull, tail ? (1u << j) : 0u);
+            __syncwarp();
+            if ((has >> lane) & 1u) {
+                sum_sq += S.sums[lane][0];
+                sum_phi += S.sums[lane][1];
+            }
+            __syncwarp();
         }
-        const bool tail = live && (lane == 31 || jnext != j);
-        if (tail) {
-            S.sums[j][0] = t[0];
-            S.sums[j][1] = t[1];
-        }
-        const unsigned has = __reduce_or_sync(kFull, tail ? (1u << j) : 0u);
-        __syncwarp();
-        if ((has >> lane) & 1u) {
-            sum_sq += S.sums[lane][0];
-            sum_phi += S.sums[lane][1];
-        }
-        __syncwarp();
     }
-    double rd = 0.0;
+    DensSums v{0.0, 0.0, 0.0, 0.0};
     if (valid) {
         float denom = sum_phi;
         if (denom < FLT_EPSILON) denom = FLT_EPSILON;
-        float re = (float)log((double)(1e-8f + sum_sq / denom));
-        dens_node[node] = make_float4(sum_phi, (float)exp((double)re), r[node], re);
-        rd = (double)re;
+        const float re = (float)log((double)(1e-8f + sum_sq / denom));
+        const float r = A.r[node];
+        A.dens_node[node] = make_float4(sum_phi, (float)exp((double)re), r, re);
+        const double red_ = (double)re, rd = (double)r;
+        v = DensSums{red_, red_ * red_, red_ * rd, rd};
     }
-    // fixed-order f64 sum: warp tree, then the block's warps in order
+    // block sums, fixed order: warp tree, then the block's warps in order
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) rd += __shfl_down_sync(kFull, rd, off);
-    if (lane == 0) shw[warp] = rd;
+    for (int off = 16; off > 0; off >>= 1) {
+        v.s_re += __shfl_down_sync(kFull, v.s_re, off);
+        v.s_re2 += __shfl_down_sync(kFull, v.s_re2, off);
+        v.s_rer += __shfl_down_sync(kFull, v.s_rer, off);
+        v.s_r += __shfl_down_sync(kFull, v.s_r, off);
+    }
+    if (lane == 0) shw[warp] = v;
     __syncthreads();
     if (threadIdx.x == 0) {
-        double acc = 0.0;
-        for (int w = 0; w < kW; w++) acc += shw[w];
-        part[blockIdx.x] = acc;
+        DensSums acc{0.0, 0.0, 0.0, 0.0};
+        for (int w = 0; w < kW; w++) {
+            acc.s_re += shw[w].s_re;
+            acc.s_re2 += shw[w].s_re2;
+            acc.s_rer += shw[w].s_rer;
+            acc.s_r += shw[w].s_r;
+        }
+        double *pp = A.part + 4ull * blockIdx.x;
+        pp[0] = acc.s_re;
+        pp[1] = acc.s_re2;
+        pp[2] = acc.s_rer;
+        pp[3] = acc.s_r;
+        __threadfence();
+        is_last = atomicAdd(A.ticket, 1u) == gridDim.x - 1;
     }
-}
-
-// mean of the log radii from the per-block partials (fixed order)
-__global__ void k_dens_mean(const double *__restrict__ part, uint32_t nparts, uint32_t n, double *__restrict__ mean)
-{
-    __shared__ double sh[1024];
-    double acc = 0.0;
-    for (uint32_t i = threadIdx.x; i < nparts; i += blockDim.x) acc += part[i];
-    sh[threadIdx.x] = acc;
     __syncthreads();
-    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-        if ((int)threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
-        __syncthreads();
+    if (!is_last) return;
+    __threadfence();
+    // the last block: every block's sums, a fixed order per thread, then a
+    // fixed tree over the threads
+    DensSums acc{0.0, 0.0, 0.0, 0.0};
+    for (uint32_t b = threadIdx.x; b < gridDim.x; b += kDensBlock) {
+        const double *pp = A.part + 4ull * b;
+        acc.s_re += __ldcg(pp);
+        acc.s_re2 += __ldcg(pp + 1);
+        acc.s_rer += __ldcg(pp + 2);
+        acc.s_r += __ldcg(pp + 3);
     }
-    if (threadIdx.x == 0) *mean = sh[0] / (double)(n > 1 ? n : 1);
-}
-
-// per-block (sum d^2, sum d * r) with d = re - mean (density.rs:483-498)
-__global__ void __launch_bounds__(kDensBlock) k_dens_moments(uint32_t n, const float4 *__restrict__ dens_node,
-                                                              const double *__restrict__ mean,
-                                                              double2 *__restrict__ part)
-{
-    __shared__ double2 sh[kDensBlock];
-    const uint32_t i = blockIdx.x * kDensBlock + threadIdx.x;
-    double2 acc = make_double2(0.0, 0.0);
-    if (i < n) {
-        float4 dn = dens_node[i];
-        double d = (double)dn.w - *mean;
-        acc = make_double2(d * d, d * (double)dn.z);
-    }
-    sh[threadIdx.x] = acc;
+    red[threadIdx.x] = acc;
     __syncthreads();
     for (int w = kDensBlock / 2; w > 0; w >>= 1) {
         if ((int)threadIdx.x < w) {
-            sh[threadIdx.x].x += sh[threadIdx.x + w].x;
-            sh[threadIdx.x].y += sh[threadIdx.x + w].y;
-        }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
-}
-
-// density.rs:500-507 + launch_dens_update's host scalars
-// (umap_optimiser_gpu.rs:1123-1142): stats = {mean, std, cov, inv_var, coeff}
-// in f32.
-__global__ void k_dens_final(const double2 *__restrict__ part, uint32_t nparts, uint32_t n,
-                             const double *__restrict__ mean, float var_shift, float lambda, float mu_tot,
-                             float *__restrict__ stats)
-{
-    __shared__ double2 sh[1024];
-    double2 acc = make_double2(0.0, 0.0);
-    for (uint32_t i = threadIdx.x; i < nparts; i += blockDim.x) {
-        acc.x += part[i].x;
-        acc.y += part[i].y;
-    }
-    sh[threadIdx.x] = acc;
-    __syncthreads();
-    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-        if ((int)threadIdx.x < w) {
-            sh[threadIdx.x].x += sh[threadIdx.x + w].x;
-            sh[threadIdx.x].y += sh[threadIdx.x + w].y;
+            red[threadIdx.x].s_re += red[threadIdx.x + w].s_re;
+            red[threadIdx.x].s_re2 += red[threadIdx.x + w].s_re2;
+            red[threadIdx.x].s_rer += red[threadIdx.x + w].s_rer;
+            red[threadIdx.x].s_r += red[threadIdx.x + w].s_r;
         }
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        double denom = (double)(n > 2 ? n - 1 : 1);
-        double var = sh[0].x / denom, cov = sh[0].y / denom;
-        double sd = sqrt(var + (double)var_shift);
-        float mean_f = (float)*mean, std_f = (float)sd, cov_f = (float)cov;
-        float inv_var = 1.0f / (std_f * std_f);
-        float dn = (float)(n > 1 ? n - 1 : 1);
-        stats[0] = mean_f;
-        stats[1] = std_f;
-        stats[2] = cov_f;
-        stats[3] = inv_var;
-        stats[4] = lambda * mu_tot / (std_f * dn);
+        const DensSums t = red[0];
+        const double nn = (double)(n > 1 ? n : 1);
+        const double denom = (double)(n > 2 ? n - 1 : 1);
+        const double mean = t.s_re / nn;
+        const double var = (t.s_re2 - t.s_re * t.s_re / nn) / denom;
+        const double cov = (t.s_rer - mean * t.s_r) / denom;
+        const double sd = sqrt(var + (double)A.var_shift);
+        const float mean_f = (float)mean, std_f = (float)sd, cov_f = (float)cov;
+        const float inv_var = 1.0f / (std_f * std_f);
+        const float dn = (float)(n > 1 ? n - 1 : 1);
+        A.stats[0] = mean_f;
+        A.stats[1] = std_f;
+        A.stats[2] = cov_f;
+        A.stats[3] = inv_var;
+        A.stats[4] = A.lambda * A.mu_tot / (std_f * dn);
+        *A.ticket = 0u;
     }
 }
 
@@ -321,11 +336,9 @@ void launch_epoch(const EpochArgs &A, uint32_t n_dim, bool dens, cudaStream_t s)
 void launch_dens_update(const DensArgs &Dn, uint32_t n_dim, cudaStream_t s)
 {
     const uint32_t nb = ceil_div(Dn.n, kDensBlock);
-#define UMAPCU_CASE(DD)                                                                                   \
-    case DD:                                                                                              \
-        k_dens_radii<DD><<<nb, kDensBlock, 0, s>>>(Dn.n, Dn.offsets, Dn.other, Dn.y, Dn.a, Dn.b, Dn.precise_pow, \
-                                                    Dn.r,                                                 \
-                                                    Dn.dens_node, Dn.part1);                              \
+#define UMAPCU_CASE(DD)                                           \
+    case DD:                                                      \
+        k_dens_update<DD><<<nb, kDensBlock, 0, s>>>(Dn);          \
         break;
     switch (n_dim) {
         UMAPCU_CASE(1) UMAPCU_CASE(2) UMAPCU_CASE(3) UMAPCU_CASE(4)
@@ -333,11 +346,7 @@ void launch_dens_update(const DensArgs &Dn, uint32_t n_dim, cudaStream_t s)
         default: fail(UMAPCU_BAD_ARG, "n_dim must be in 1..8");
     }
 #undef UMAPCU_CASE
-    check_launch("k_dens_radii");
-    k_dens_mean<<<1, 1024, 0, s>>>(Dn.part1, nb, Dn.n, Dn.mean);
-    k_dens_moments<<<nb, kDensBlock, 0, s>>>(Dn.n, Dn.dens_node, Dn.mean, Dn.part2);
-    k_dens_final<<<1, 1024, 0, s>>>(Dn.part2, nb, Dn.n, Dn.mean, Dn.var_shift, Dn.lambda, Dn.mu_tot, Dn.stats);
-    check_launch("k_dens_final");
+    check_launch("k_dens_update");
 }
 
 uint32_t dens_partials(uint32_t n) { return ceil_div(n, kDensBlock); }

@@ -49,9 +49,8 @@ struct DensArgs {
     float a, b;
     const float *r;       // [n] z-scored original log radii
     float4 *dens_node;    // [n] output
-    double *part1;        // [dens_partials(n)]
-    double2 *part2;       // [dens_partials(n)]
-    double *mean;         // [1]
+    double *part;         // [4 * dens_partials(n)] per-block f64 sums
+    uint32_t *ticket;     // [1] zero between launches (the last block re-arms it)
     float *stats;         // [5]
     float var_shift, lambda, mu_tot;
     bool precise_pow;

@@ -574,6 +574,13 @@ void umapcu_server::loop()
 
 extern "C" {
 
+umapcu_status umapcu_server_job_bytes(uint32_t n, uint32_t n_dim, uint64_t nnz, uint32_t n_epochs, uint64_t *bytes)
+{
+    if (!bytes) return UMAPCU_BAD_ARG;
+    *bytes = job_bytes(n, n_dim, nnz, n_epochs);
+    return UMAPCU_OK;
+}
+
 umapcu_status umapcu_server_create(uint64_t device_budget_bytes, uint32_t max_jobs, uint32_t tick_epochs,
                                    uint32_t n_dim, umapcu_server **out)
 {

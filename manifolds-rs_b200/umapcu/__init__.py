@@ -159,6 +159,9 @@ _SIGS = {
     "umapcu_set_pool_retention": [_i32],
     "umapcu_release_cached": [],
     "umapcu_probe_l2_gather": [_u64, _vp],
+    "umapcu_device_count": [_vp],
+    "umapcu_server_job_bytes": [_u32, _u32, _u64, _u32, _vp],
+    "umapcu_set_device": [_i32],
 }
 for _name, _args in _SIGS.items():
     _fn = getattr(_lib, _name)
@@ -745,6 +748,26 @@ def release_cached():
     """Frees the current device's cached schedule-bitmask block and trims its
     default memory pool."""
     _check(_lib.umapcu_release_cached(), "release_cached")
+
+
+def server_job_bytes(n: int, n_dim: int, nnz: int, n_epochs: int) -> int:
+    """Device bytes a server's admission charges for a job (its budget unit)."""
+    b = C.c_uint64()
+    _check(_lib.umapcu_server_job_bytes(n, n_dim, nnz, n_epochs, C.byref(b)))
+    return b.value
+
+
+def device_count() -> int:
+    """Visible CUDA devices (0 without a driver or device)."""
+    c = C.c_int()
+    st = _lib.umapcu_device_count(C.byref(c))
+    return c.value if st == OK else 0
+
+
+def set_device(device: int):
+    """Makes `device` the calling thread's current device for the library's
+    entry points (states, batches and servers bind to it when created)."""
+    _check(_lib.umapcu_set_device(int(device)), "set_device")
 
 
 def probe_l2_gather(table_bytes: int = 8 << 20) -> float:

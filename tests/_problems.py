@@ -53,3 +53,57 @@ def oracle_adam_gpu_run(args):
     if st != O.OK:
         raise RuntimeError(f"oracle status {st}")
     return yo
+
+
+# The benchmark workloads' inputs (the shapes BASELINE's configurations name):
+# name -> (n, dim, clusters, k, n_epochs, generator), data seed 2024.
+CONFIGS = {
+    "c1": (10_000, 50, 10, 15, 500, "isotropic"),
+    "c2": (1_000_000, 50, 30, 15, 200, "anisotropic"),
+    "c3": (200_000, 30, 20, 30, 200, "variable"),
+}
+
+
+@functools.lru_cache(maxsize=3)
+def config_inputs(name, seed=2024):
+    """(X, knn_idx, knn_dist) of a benchmark workload. The exact kNN comes
+    from the library's GPU brute force (bit-exact with the oracle's, see
+    test_gpu_knn.py) and is kept in a kNN cache file under the temp
+    directory (UMAPCU_TEST_KNN_CACHE overrides), written and read with the
+    NumPy cache reader."""
+    import os
+    import tempfile
+
+    import umapcu
+    import umapdata.synth as S
+    from umapdata import knn_cache
+    n, dim, clusters, k, _, kind = CONFIGS[name]
+    gen = {"isotropic": S.isotropic_mixture, "anisotropic": S.anisotropic_mixture,
+           "variable": S.variable_density_mixture}[kind]
+    X, _ = gen(n, dim, clusters, seed)
+    d = os.environ.get("UMAPCU_TEST_KNN_CACHE") or os.path.join(tempfile.gettempdir(), "umapcu_test_knn")
+    os.makedirs(d, exist_ok=True)
+    path = os.path.join(d, f"{name}_s{seed}_exact.knn")
+    if os.path.exists(path):
+        try:
+            idx, dist, _ = knn_cache.load(path)
+            if idx.shape == (n, k):
+                return X, idx, dist
+        except ValueError:
+            pass
+    idx, dist = umapcu.knn_exact(X, k)
+    tmp = f"{path}.{os.getpid()}.tmp"
+    knn_cache.save(tmp, idx, dist)
+    os.replace(tmp, path)
+    return X, idx, dist
+
+
+@functools.lru_cache(maxsize=3)
+def config_oracle_graph(name, seed=2024):
+    """The oracle's fuzzy graph of a benchmark workload, with its sigma/rho
+    and adjacency row pointers."""
+    X, idx, dist = config_inputs(name, seed)
+    n, _, _, _, n_epochs, _ = CONFIGS[name]
+    (r, c, v), sig, rho = O.construct_umap_graph(idx, dist, n_epochs)
+    return dict(X=X, idx=idx, dist=dist, row=r, col=c, val=v, sigma=sig, rho=rho, ptr=O.coo_to_adj_ptr(n, r),
+                n=n, n_epochs=n_epochs)

@@ -1,0 +1,146 @@
+"""The north-star full-run bar at the benchmark workloads' sizes (needs a
+B200): trustworthiness@15, kNN preservation@15 and fuzzy cross-entropy of
+the CUDA optimiser's final embedding within 1 % of the oracle's restatement
+of the reference's GPU optimiser (optimise_embedding_adam_gpu,
+umap_optimiser_gpu.rs:1302-1369), on the same fuzzy graph, the same initial
+embedding and the same negative sampler (gpu_hash_neg, :611-624).
+
+A run's trajectory departs from any other run's at the f32 rounding level
+and then diverges chaotically, so single runs differ by the seed-to-seed
+spread of the metrics. The bar is therefore applied to means over seed
+ensembles (the sampler seed varies, the initial embedding is fixed), sized
+so that their standard errors sit well below 1 %:
+
+* C1, 10k x 50, 10 isotropic Gaussians, k = 15, 500 epochs: 48 seeds per
+  side, every metric over all points;
+* C3, 200k x 30, 20 clusters of different spread, k = 30, 200 epochs with
+  the densMAP term in the last 30 %: 8 seeds per side;
+* C2, 1M x 50, 30 anisotropic components, k = 15, 200 epochs: one oracle run
+  (tens of seconds on the host cores) against the mean of 4 GPU runs.
+
+trust and kNN preservation on C2 and C3 are evaluated on a seeded 10 000-query
+subsample against all points, the same queries on both sides. The measured
+means, spreads and differences are printed (pytest -s) for the record.
+"""
+import multiprocessing as mp
+import os
+from concurrent.futures import ProcessPoolExecutor
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests._problems import config_oracle_graph
+
+pytestmark = pytest.mark.gpu
+
+umapcu = pytest.importorskip("umapcu")
+
+
+def _oracle_run(args):
+    """One oracle run (process-pool worker): -> final embedding."""
+    init, ptr, col, val, pd, seed, dens = args
+    st, yo = O.optimise_adam_gpu(init, init.shape[0], ptr, col, val, pd, seed, dens)
+    if st != O.OK:
+        raise RuntimeError(f"oracle status {st}")
+    return yo
+
+
+def _oracle_runs(g, init, p, seeds, dens, procs):
+    jobs = [(init, g["ptr"], g["col"], g["val"], p.as_dict(), s, dens) for s in seeds]
+    if procs <= 1:
+        return [_oracle_run(j) for j in jobs]
+    old = os.environ.get("OMP_NUM_THREADS")
+    os.environ["OMP_NUM_THREADS"] = str(max(1, (os.cpu_count() or 1) // procs))
+    try:
+        with ProcessPoolExecutor(procs, mp_context=mp.get_context("spawn")) as ex:
+            return list(ex.map(_oracle_run, jobs))
+    finally:
+        if old is None:
+            del os.environ["OMP_NUM_THREADS"]
+        else:
+            os.environ["OMP_NUM_THREADS"] = old
+
+
+def _metrics(g, Y, p, queries):
+    q = umapcu.embedding_quality(g["X"], Y, g["idx"].astype(np.int32)[:, :15], 15, queries=queries)
+    coo = umapcu.CoordinateList(g["row"], g["col"], g["val"], g["n"])
+    return np.array([q["trust"], q["knn_preservation"], umapcu.fuzzy_cross_entropy(coo, Y, p.a, p.b)])
+
+
+def _compare(name, mg, mo):
+    """Means of the two ensembles within 1 % per metric; prints the record."""
+    mg, mo = np.atleast_2d(mg), np.atleast_2d(mo)
+    a, b = mg.mean(0), mo.mean(0)
+    sg = mg.std(0, ddof=1) if len(mg) > 1 else np.full(3, np.nan)
+    so = mo.std(0, ddof=1) if len(mo) > 1 else np.full(3, np.nan)
+    rel = np.abs(a - b) / np.abs(b)
+    for i, key in enumerate(("trust15", "knn_preservation15", "fuzzy_ce")):
+        print(f"[fullrun {name}] {key}: gpu {a[i]:.6g} (sd {sg[i]:.3g}, n {len(mg)}) oracle {b[i]:.6g} "
+              f"(sd {so[i]:.3g}, n {len(mo)}) rel diff {rel[i]:.4%}")
+    for i, key in enumerate(("trust15", "knn_preservation15", "fuzzy_ce")):
+        assert rel[i] <= 0.01, (name, key, a[i], b[i])
+
+
+def _queries(n, seed=77):
+    if n <= 20_000:
+        return None
+    return np.sort(np.random.default_rng(seed).choice(n, 10_000, replace=False)).astype(np.uint32)
+
+
+def test_full_run_quality_c1():
+    g = config_oracle_graph("c1")
+    n = g["n"]
+    p = umapcu.UmapOptimParams.from_min_dist_spread(0.1, 1.0, n_epochs=500, neg_sample_rate=5)
+    init = umapcu.random_layout(n, 2, 2024)
+    adj = umapcu.Adjacency(g["ptr"], g["col"], g["val"])
+    seeds = list(range(48))
+    mg = []
+    for s in seeds:
+        y = init.copy()
+        umapcu.optimise_embedding_adam_gpu(y, adj, p, None, s)
+        assert np.isfinite(y).all()
+        mg.append(_metrics(g, y, p, None))
+    yos = _oracle_runs(g, init, p, seeds, None, min(16, os.cpu_count() or 1))
+    mo = [_metrics(g, y, p, None) for y in yos]
+    _compare("c1", mg, mo)
+
+
+def test_full_run_quality_c3_densmap():
+    g = config_oracle_graph("c3")
+    n = g["n"]
+    coo = umapcu.CoordinateList(g["row"], g["col"], g["val"], n)
+    dens = umapcu.DensState.new(umapcu.DensParams(), coo, g["idx"], g["dist"], True)
+    dd = {"r": dens.r, "lambda": dens.params.lambda_, "frac": dens.params.frac, "var_shift": dens.params.var_shift,
+          "mu_tot": dens.mu_tot}
+    p = umapcu.UmapOptimParams.from_min_dist_spread(0.1, 1.0, n_epochs=200, neg_sample_rate=5)
+    init = umapcu.random_layout(n, 2, 2024)
+    adj = umapcu.Adjacency(g["ptr"], g["col"], g["val"])
+    seeds = list(range(8))
+    qs = _queries(n)
+    mg = []
+    for s in seeds:
+        y = init.copy()
+        umapcu.optimise_embedding_adam_gpu(y, adj, p, dens, s)
+        assert np.isfinite(y).all()
+        mg.append(_metrics(g, y, p, qs))
+    yos = _oracle_runs(g, init, p, seeds, dd, min(8, os.cpu_count() or 1))
+    mo = [_metrics(g, y, p, qs) for y in yos]
+    _compare("c3", mg, mo)
+
+
+def test_full_run_quality_c2():
+    g = config_oracle_graph("c2")
+    n = g["n"]
+    p = umapcu.UmapOptimParams.from_min_dist_spread(0.1, 1.0, n_epochs=200, neg_sample_rate=5)
+    init = umapcu.random_layout(n, 2, 2024)
+    adj = umapcu.Adjacency(g["ptr"], g["col"], g["val"])
+    qs = _queries(n)
+    mg = []
+    for s in range(4):
+        y = init.copy()
+        umapcu.optimise_embedding_adam_gpu(y, adj, p, None, s)
+        assert np.isfinite(y).all()
+        mg.append(_metrics(g, y, p, qs))
+    yo = _oracle_runs(g, init, p, [0], None, 1)[0]
+    _compare("c2", mg, [_metrics(g, yo, p, qs)])
