@@ -554,43 +554,62 @@ def init_group(world, backend="nccl"):
     return dist
 
 
-def make_batch_problems(wl, seed):
-    """The C4 problem set: seeded sizes, data, exact kNN, CUDA graph stage."""
-    import umapcu
-    import umapdata.synth as S
+def batch_problem_sizes(wl, seed):
+    """The C4 problem set's sizes and cluster counts (seeded; the same in
+    every rank)."""
     rng = np.random.default_rng(seed)
     sizes = np.exp(rng.uniform(np.log(wl["n_lo"]), np.log(wl["n_hi"]), wl["problems"])).astype(int)
+    clusters = rng.integers(wl["clusters"][0], wl["clusters"][1] + 1, wl["problems"])
+    return sizes, clusters
+
+
+def make_batch_problems(wl, seed, which):
+    """Problems `which` of the C4 set: seeded data, exact kNN, CUDA graph
+    stage, seeded initial layout (each problem's inputs depend only on its
+    own index)."""
+    import umapcu
+    import umapdata.synth as S
+    sizes, clusters = batch_problem_sizes(wl, seed)
     adjs, inits = [], []
     t0 = time.time()
-    for i, n in enumerate(sizes):
-        X, _ = S.isotropic_mixture(int(n), wl["dim"], int(rng.integers(wl["clusters"][0], wl["clusters"][1] + 1)),
-                                   seed + 1000 + i)
-        idx, dist = umapcu.knn_exact(X, wl["k"])
-        g = umapcu.construct_umap_graph(idx, dist, umapcu.UmapGraphParams(), wl["n_epochs"])
+    for i in which:
+        n = int(sizes[i])
+        X, _ = S.isotropic_mixture(n, wl["dim"], int(clusters[i]), seed + 1000 + i)
+        idx, knn_d = umapcu.knn_exact(X, wl["k"])
+        g = umapcu.construct_umap_graph(idx, knn_d, umapcu.UmapGraphParams(), wl["n_epochs"])
         adjs.append(umapcu.coo_to_adjacency_list(g))
-        inits.append(umapcu.random_layout(int(n), 2, seed + 5000 + i))
-    log(f"[bench] {len(sizes)} problems, {int(sizes.sum())} points, prepared in {time.time() - t0:.1f}s")
-    return sizes, adjs, inits
+        inits.append(S.random_layout(n, 2, seed + 5000 + i))
+    log(f"[bench] {len(which)} problems, {int(sizes[which].sum())} points, prepared in {time.time() - t0:.1f}s")
+    return sizes[which], adjs, inits
 
 
 def run_batched(args, wl, world, rank, local_rank):
-    """Batched form vs sequential single-problem runs, embeddings/s; every
-    rank runs its own problem set, times are the max over ranks."""
+    """Batched form vs sequential single-problem runs, embeddings/s. With
+    several ranks the 512 problems are placed over the GPUs by
+    umapcu.pool.lpt_partition on their sizes (the same placement in every
+    rank, no data exchange); each rank runs one batch of its share and the
+    time is the max over ranks (strong scaling: the problem set is fixed)."""
     import torch
     import umapcu
+    from umapcu.pool import lpt_partition
     torch.cuda.set_device(local_rank)
-    dist = init_group(world)
-    seed = args.seed + rank
-    sizes, adjs, inits = make_batch_problems(wl, seed)
+    group = init_group(world)
+    seed = args.seed
+    all_sizes, _ = batch_problem_sizes(wl, seed)
+    shares = lpt_partition(all_sizes.astype(np.float64), world)
+    mine = shares[rank]
+    sizes, adjs, inits = make_batch_problems(wl, seed, mine)
     params = umapcu.UmapOptimParams.from_min_dist_spread(0.1, 1.0, n_epochs=wl["n_epochs"], neg_sample_rate=5)
-    seeds = [seed + i for i in range(len(sizes))]
+    seeds = [seed + i for i in mine]
     B = umapcu.UmapBatch(inits, adjs, params, seeds)
     cfg = B.autotune()
     for _ in range(args.warmup):
         B.run(0)
+    if group:
+        group.barrier()
     with ClockSampler(local_rank) as clk:
         ms = [B.run(0) for _ in range(args.steps)]
-    t_batch = max_over_ranks(float(np.sum(ms)) / 1e3, dist)
+    t_batch = max_over_ranks(float(np.sum(ms)) / 1e3, group)
     # edge-updates per run, from each problem's periods
     updates = 0
     states = []
@@ -615,7 +634,7 @@ def run_batched(args, wl, world, rank, local_rank):
         st.run(0, wl["n_epochs"])
     e1.record(stream)
     torch.cuda.synchronize()
-    t_seq = max_over_ranks(e0.elapsed_time(e1) / 1e3, dist)
+    t_seq = max_over_ranks(e0.elapsed_time(e1) / 1e3, group)
     # identical results in the batch and alone (spot check)
     ok = True
     for i in (0, len(sizes) // 2, len(sizes) - 1):
@@ -623,17 +642,18 @@ def run_batched(args, wl, world, rank, local_rank):
         ok &= bool(np.array_equal(B.read(i), y_single))
     for st in states:
         st.close()
-    P = len(sizes)
-    value = world * args.steps * P / t_batch
+    updates = max_over_ranks(updates, group) if group is None else _sum_over_ranks(updates, group)
+    P = len(all_sizes)
+    value = args.steps * P / t_batch
     out = {"metric": "UMAP batched embeddings/s (512 problems)", "value": value, "unit": "embeddings/s",
            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-           "ms_per_step": round(t_batch / args.steps * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+           "ms_per_step": round(t_batch / args.steps * 1e3, 3), "higher_is_better": True, "scaling": "strong",
            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-           "config": {"workload": f"c4: {wl['desc']}", "problems": P, "points": int(sizes.sum()),
+           "config": {"workload": f"c4: {wl['desc']}", "problems": P, "points": int(all_sizes.sum()),
+                      "placement": f"LPT over {world} GPU(s) by problem size; this rank {len(mine)} problems",
                       "autotuned": cfg, "l2": "not flushed (state reset kernel precedes every run)"},
-           "edge_updates_per_s": world * args.steps * updates / t_batch,
+           "edge_updates_per_s": args.steps * updates / t_batch,
            "sequential_plain": {"embeddings_per_s": P / t_seq, "ms": round(t_seq * 1e3, 3)},
-           "sequential_plain_total": {"embeddings_per_s": world * P / t_seq},
            "speedup_vs_sequential": round((P / t_batch * args.steps) / (P / t_seq), 2) if t_seq > 0 else None,
            "same_result_alone_and_batched": ok,
            # per run: the state reset kernel, then one persistent launch or one launch per epoch
@@ -642,20 +662,44 @@ def run_batched(args, wl, world, rank, local_rank):
     if rank == 0:
         print(json.dumps(out), flush=True)
     B.close()
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    if group:
+        group.barrier()
+        group.destroy_process_group()
+
+
+def _sum_over_ranks(x, group):
+    import torch
+    dev = "cuda" if group.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], device=dev, dtype=torch.float64)
+    group.all_reduce(t)
+    return float(t.item())
+
+
+def place_requests(work, world):
+    """Online placement of a request stream over ranks: each request, in
+    arrival order, to the rank with the least work placed so far (ties: the
+    lowest rank). Deterministic, so every rank derives the same assignment."""
+    load = np.zeros(world)
+    out = np.empty(len(work), np.int64)
+    for r, w in enumerate(work):
+        k = int(np.argmin(load))
+        out[r] = k
+        load[k] += w
+    return out
 
 
 def run_served(args, wl, world, rank, local_rank):
-    """Continuous-batching server under a Poisson request stream; every rank
-    serves its own stream, the span is the max over ranks."""
+    """Continuous-batching server under a Poisson request stream. With
+    several ranks one stream of world x requests at world x the rate is
+    placed over the GPUs by place_requests (least work placed so far, the
+    same assignment in every rank); each rank's server takes its share at
+    the requests' arrival times; the span is the max over ranks."""
     import torch
     import umapcu
     import umapdata.synth as S
     torch.cuda.set_device(local_rank)
-    dist = init_group(world)
-    seed = args.seed + rank
+    group = init_group(world)
+    seed = args.seed
     rng = np.random.default_rng(seed)
     t0 = time.time()
     pool = []
@@ -663,25 +707,27 @@ def run_served(args, wl, world, rank, local_rank):
         n = int(np.exp(rng.uniform(np.log(wl["n_lo"]), np.log(wl["n_hi"]))))
         dim = int(rng.choice(wl["dims"]))
         X, _ = S.isotropic_mixture(n, dim, int(rng.integers(wl["clusters"][0], wl["clusters"][1] + 1)), seed + 70 + i)
-        idx, dist = umapcu.knn_exact(X, wl["k"])
-        g = umapcu.construct_umap_graph(idx, dist, umapcu.UmapGraphParams(), wl["n_epochs"])
+        idx, knn_d = umapcu.knn_exact(X, wl["k"])
+        g = umapcu.construct_umap_graph(idx, knn_d, umapcu.UmapGraphParams(), wl["n_epochs"])
         pool.append(umapcu.coo_to_adjacency_list(g))
     log(f"[bench] served pool of {len(pool)} graphs prepared in {time.time() - t0:.1f}s")
     params = umapcu.UmapOptimParams.from_min_dist_spread(0.1, 1.0, n_epochs=wl["n_epochs"], neg_sample_rate=5)
-    n_req = args.requests or wl["requests"]
+    n_req = (args.requests or wl["requests"]) * world
     req_graph = rng.integers(0, len(pool), n_req)
+    owner = place_requests([pool[int(g)].col.size for g in req_graph], world)
 
     def init_of(r):
         g = int(req_graph[r])
-        return umapcu.random_layout(pool[g].n, 2, seed + 9000 + r)
+        return S.random_layout(pool[g].n, 2, seed + 9000 + r)
 
     # capacity: the server's own steady-state throughput under a saturating
     # burst (every request submitted at once; admission, graph builds and
     # ticks included), embeddings/s for this size mix, taken between the
-    # 10th and 90th percentile completions (ramp-up and drain excluded)
+    # 10th and 90th percentile completions (ramp-up and drain excluded); the
+    # slowest rank's figure sets the stream's rate
     n_cal = 20 * len(pool)
     cal_rng = np.random.default_rng(seed + 5)
-    cal = [(pool[int(g)], umapcu.random_layout(pool[int(g)].n, 2, seed + 7000 + i))
+    cal = [(pool[int(g)], S.random_layout(pool[int(g)].n, 2, seed + 7000 + i))
            for i, g in enumerate(cal_rng.integers(0, len(pool), n_cal))]
     sv = umapcu.UmapServer(budget_bytes=wl["budget"], max_jobs=4096, tick_epochs=10, n_dim=2)
     for g, y0 in cal[:len(pool)]:  # warm-up
@@ -689,21 +735,24 @@ def run_served(args, wl, world, rank, local_rank):
     subs = []
     for i, (g, y0) in enumerate(cal):
         subs.append((time.perf_counter(), sv.submit(y0, g, params, seed=i)))
-    done = np.sort([t0 + sv.wait(t)[1] for t0, t in subs])
+    done = np.sort([ts + sv.wait(t)[1] for ts, t in subs])
     lo, hi = int(0.1 * n_cal), int(0.9 * n_cal)
     cap = (hi - lo) / (done[hi] - done[lo])
     sv.close()
-    lam = wl["util"] * cap
+    cap = -max_over_ranks(-cap, group)  # the minimum over ranks
+    lam = world * wl["util"] * cap
     gaps = rng.exponential(1.0 / lam, n_req)
-    inits = [init_of(r) for r in range(n_req)]  # client-side data, made before the stream starts
+    arrive = np.cumsum(gaps)
+    mine = [r for r in range(n_req) if owner[r] == rank]
+    inits = {r: init_of(r) for r in mine}  # client-side data, made before the stream starts
     sv = umapcu.UmapServer(budget_bytes=wl["budget"], max_jobs=4096, tick_epochs=10, n_dim=2)
     tickets = []
+    if group:
+        group.barrier()
     t_start = time.perf_counter()
-    t_next = t_start
     with ClockSampler(local_rank) as clk:
-        for r in range(n_req):
-            t_next += gaps[r]
-            d = t_next - time.perf_counter()
+        for r in mine:
+            d = t_start + arrive[r] - time.perf_counter()
             if d > 0:
                 time.sleep(d)
             tickets.append(sv.submit(inits[r], pool[int(req_graph[r])], params, seed=seed + r))
@@ -716,14 +765,20 @@ def run_served(args, wl, world, rank, local_rank):
         t_end = time.perf_counter()
     st = sv.stats()
     sv.close()
-    span = max_over_ranks(t_end - t_start, dist)
-    out = {"metric": "UMAP served embeddings/s (Poisson stream)", "value": world * n_req / span,
+    span = max_over_ranks(t_end - t_start, group)
+    if group:
+        every = [None] * world
+        group.all_gather_object(every, (lat, queue))
+        lat = [x for a, _ in every for x in a]
+        queue = [x for _, b in every for x in b]
+    out = {"metric": "UMAP served embeddings/s (Poisson stream)", "value": n_req / span,
            "unit": "embeddings/s",
            "n_gpus": world, "steps": 1, "warmup": 0, "ms_per_step": round(span * 1e3, 3),
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
            "config": {"workload": f"c5: {wl['desc']}", "requests": n_req, "arrival_rate_per_s": round(lam, 2),
-                      "submitted_rate_per_s": round(n_req / (t_sub - t_start), 2),
-                      "capacity_per_s": round(cap, 2),
+                      "submitted_rate_per_s_rank0": round(len(mine) / max(t_sub - t_start, 1e-9), 2),
+                      "capacity_per_s_per_gpu": round(cap, 2),
+                      "placement": f"least work placed so far, over {world} GPU(s)",
                       "budget_bytes": wl["budget"], "tick_epochs": 10},
            "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                          "mean": float(np.mean(lat)), "max": float(np.max(lat))},
@@ -731,9 +786,9 @@ def run_served(args, wl, world, rank, local_rank):
            "server": st, "clocks": clk.summary()}
     if rank == 0:
         print(json.dumps(out), flush=True)
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    if group:
+        group.barrier()
+        group.destroy_process_group()
 
 
 def run_spectral(args, wl, world, rank, local_rank):

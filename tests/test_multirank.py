@@ -1,8 +1,9 @@
 """bench.py's multi-rank host logic on CPU (no GPU): the timed region's
-max over ranks on a 2-rank gloo group, and the reference arm's non-zero
-ranks, which leave without work or output. The plain path runs as
-independent replicas per rank, so the timing reduction is its only
-collective."""
+max over ranks (and the sum and minimum the batched and served forms use)
+on a 2-rank gloo group, the served form's request placement (the same in
+every rank without an exchange), and the reference arm's non-zero ranks,
+which leave without work or output. The plain path runs as independent
+replicas per rank, so these reductions are its only collectives."""
 import os
 import socket
 import subprocess
@@ -31,8 +32,16 @@ def _rank_main(rank, world, port, out_dir):
     try:
         got = bench.max_over_ranks(1.5 + rank, dist)
         none = bench.max_over_ranks(0.25, None)
+        tot = bench._sum_over_ranks(10.0 + rank, dist)
+        lowest = -bench.max_over_ranks(-(3.0 + rank), dist)
+        # the served form's placement of one request stream: every rank
+        # derives the same owner for every request, without an exchange
+        owner = bench.place_requests([5, 1, 1, 7, 2, 2, 9, 1], world)
+        mine = [r for r in range(8) if owner[r] == rank]
+        every = [None] * world
+        dist.all_gather_object(every, owner.tolist())
         with open(os.path.join(out_dir, f"r{rank}.txt"), "w") as f:
-            f.write(f"{got} {none}")
+            f.write(f"{got} {none} {tot} {lowest} {int(every[0] == every[1])} {len(mine)}")
         dist.barrier()
     finally:
         dist.destroy_process_group()
@@ -42,9 +51,12 @@ def test_max_over_ranks_gloo(tmp_path):
     world = 2
     mp.start_processes(_rank_main, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True,
                        start_method="spawn")
+    counts = 0
     for r in range(world):
-        got, none = (float(x) for x in open(tmp_path / f"r{r}.txt").read().split())
-        assert got == 2.5 and none == 0.25
+        got, none, tot, lowest, same, mine = (float(x) for x in open(tmp_path / f"r{r}.txt").read().split())
+        assert got == 2.5 and none == 0.25 and tot == 21.0 and lowest == 3.0 and same == 1
+        counts += mine
+    assert counts == 8
 
 
 @pytest.mark.parametrize("rank", [1, 3])

@@ -133,3 +133,17 @@ def test_batch_pool_partition_and_read_back():
     assert pool.run() == [1.0, 1.0, 1.0]
     for i in range(P):
         assert np.array_equal(pool.read(i), embds[i] + np.float32(i))
+
+
+def test_request_placement_least_work_first():
+    import os
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+    owner = bench.place_requests([10, 1, 1, 1, 1, 10, 5], 2)
+    assert owner.tolist() == [0, 1, 1, 1, 1, 1, 0]
+    rng = np.random.default_rng(1)
+    w = rng.integers(1, 100, 2000)
+    o = bench.place_requests(w, 4)
+    loads = [w[o == k].sum() for k in range(4)]
+    assert max(loads) - min(loads) <= w.max()
