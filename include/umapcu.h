@@ -333,10 +333,15 @@ void umapcu_server_destroy(umapcu_server *sv);
  * launched. All scratch (Adam moments, the second embedding buffer,
  * schedule cursors) lives in one 16 MiB device array that every GPU loading
  * the library holds until exit: a call needs 8 * n_entries + 12 * n * n_dim
- * bytes (each part rounded up to 256) and larger problems return
- * UMAPCU_CAPACITY. The array is shared by every call on a device and keeps
- * the last call's contents (each call re-initialises what it reads); calls
- * that overlap on the GPU race on it. The first call on a device looks the
+ * bytes (each part rounded up to 256) of its first 16 MiB - 256 bytes, and
+ * larger problems return UMAPCU_CAPACITY. The array is shared by every call
+ * on a device and keeps the last call's contents (each call re-initialises
+ * what it reads); calls that overlap on the GPU race on it. The library
+ * built with UMAPCU_CHECKED (libumapcu_checked.so) also bounds-checks the
+ * caller's CSR on the device (offsets in order and within n_entries, other
+ * endpoints below n), skips any access outside it, returns UMAPCU_BAD_ARG,
+ * and for that waits for the epochs before returning. The first call on a
+ * device looks the
  * array's device address up (cudaGetSymbolAddress) and, under CUDA's default
  * lazy module loading, is also when the library's device code and this
  * array are loaded onto that device, which takes device memory: make one

@@ -47,6 +47,7 @@ struct umapcu_state {
     // csr.sched then lag (sched_lazy) until something needs them
     ScheduleLists lists;
     ScheduleBits bits;  // the bitmask form, used when there are no lists
+    DevBuf<uint32_t> err;  // checked builds: a kernel's report of a bad index
     bool lists_ok = false, bits_ok = false, sched_continuous = true, sched_lazy = false;
     uint32_t sched_epoch = 0;
     float lists_build_ms = 0.0f;
@@ -101,6 +102,8 @@ void dens_update(umapcu_state *st)
     D.lambda = st->lambda;
     D.mu_tot = st->mu_tot;
     D.precise_pow = st->precise_pow;
+    D.n_entries = 2 * st->csr.n_edges;
+    D.err = st->err.p;
     launch_dens_update(D, st->n_dim, st->stream.s);
 }
 
@@ -110,6 +113,22 @@ void sync_cursors(umapcu_state *st)
     if (!st->sched_lazy) return;
     materialise_schedule(st->csr, st->sched_epoch, st->stream.s);
     st->sched_lazy = false;
+}
+
+// Checked builds: the status a kernel reported since the last look (the
+// word is cleared); other builds: UMAPCU_OK without touching the device.
+umapcu_status take_error(umapcu_state *st)
+{
+#ifdef UMAPCU_CHECKED
+    uint32_t h = 0;
+    d2h(&h, st->err.p, 1, st->stream.s);
+    check_cuda(cudaMemsetAsync(st->err.p, 0, sizeof(uint32_t), st->stream.s), "memset err");
+    sync(st->stream.s);
+    return (umapcu_status)h;
+#else
+    (void)st;
+    return UMAPCU_OK;
+#endif
 }
 
 void run_epoch(umapcu_state *st, uint32_t epoch, uint32_t optimiser, const uint32_t *d_inj, float *d_grad,
@@ -164,6 +183,8 @@ void run_epoch(umapcu_state *st, uint32_t epoch, uint32_t optimiser, const uint3
     A.fastmod_M = fastmod_magic(st->n);
     A.optimiser = optimiser;
     A.precise_pow = st->precise_pow;
+    A.n_entries = 2 * st->csr.n_edges;
+    A.err = st->err.p;
     launch_epoch(A, st->n_dim, dens_on, st->stream.s);
     st->cur ^= 1;
 }
@@ -238,6 +259,8 @@ umapcu_status create_state(const float *embd, uint32_t n, uint32_t n_dim, const 
         st->bits_ok = build_schedule_bits(st->csr, params->n_epochs, st->bits, s);
         T.mark("schedule bitmasks", s);
     }
+    st->err.alloc(1, s);
+    check_cuda(cudaMemsetAsync(st->err.p, 0, sizeof(uint32_t), s), "memset err");
     const uint64_t nt = (uint64_t)n * n_dim;
     st->y[0].alloc(nt, s);
     st->y[1].alloc(nt, s);
@@ -359,7 +382,11 @@ const char *umapcu_status_string(umapcu_status s)
     return "unknown status";
 }
 
-const char *umapcu_version(void) { return "umapcu 0.1.0 sm_100a"; }
+#ifdef UMAPCU_CHECKED
+const char *umapcu_version(void) { return "umapcu 0.2.0 sm_100a checked"; }
+#else
+const char *umapcu_version(void) { return "umapcu 0.2.0 sm_100a"; }
+#endif
 
 // fit_params (src/training/umap_optimisers.rs:139-209), T = f32
 umapcu_status umapcu_fit_ab(float min_dist, float spread, float *a_out, float *b_out)
@@ -541,7 +568,7 @@ umapcu_status umapcu_state_run(umapcu_state *st, uint32_t first_epoch, uint32_t 
         if (!st || optimiser > UMAPCU_OPT_SGD) return UMAPCU_BAD_ARG;
         for (uint32_t e = first_epoch; e < first_epoch + count; e++) run_epoch(st, e, optimiser, nullptr, nullptr, nullptr);
         sync(st->stream.s);
-        return UMAPCU_OK;
+        return take_error(st);
     });
 }
 
@@ -575,7 +602,7 @@ umapcu_status umapcu_state_epoch_debug(umapcu_state *st, uint32_t epoch, uint32_
         if (grad) d2h(grad, g.p, (uint64_t)st->n * st->n_dim, s);
         if (has_update) d2h(has_update, act.p, st->n, s);
         sync(s);
-        return UMAPCU_OK;
+        return take_error(st);
     });
 }
 
@@ -718,7 +745,7 @@ umapcu_status umapcu_state_dens_update(umapcu_state *st, float *re, float *phi_s
         sync(s);
         if (coeff) *coeff = h[4];
         if (stats3) { stats3[0] = h[0]; stats3[1] = h[1]; stats3[2] = h[2]; }
-        return UMAPCU_OK;
+        return take_error(st);
     });
 }
 
@@ -756,7 +783,7 @@ umapcu_status umapcu_optimise_embedding(float *embd, uint32_t n, uint32_t n_dim,
         d2h(embd, st->y[st->cur].p, nt, st->stream.s);
         sync(st->stream.s);
         T.mark("embedding D2H", st->stream.s);
-        return UMAPCU_OK;
+        return take_error(st.get());
     });
 }
 

@@ -45,9 +45,12 @@ __device__ __forceinline__ uint32_t ld_acquire(const uint32_t *p)
 }
 
 // Arguments of epoch e of problem P (e counts from the problem's own start).
-__device__ __forceinline__ void epoch_args_of(const BatchProblem &P, uint32_t e, uint32_t optimiser, EpochArgs &A)
+__device__ __forceinline__ void epoch_args_of(const BatchProblem &P, uint32_t e, uint32_t optimiser, uint32_t *err,
+                                              EpochArgs &A)
 {
     A.n = P.n;
+    A.n_entries = P.n_entries;
+    A.err = err;  // checked builds report a bad index in the launch's status word
     A.offsets = P.offsets;
     A.other = P.other;
     A.sched = P.sched;
@@ -113,7 +116,7 @@ __global__ void __launch_bounds__(kWarps * 32, 8) k_batch_persistent(const Batch
         if (ej < P.n_epochs) {
             if (lane == 0) {
                 EpochArgs A{};
-                epoch_args_of(P, ej, B.optimiser, A);
+                epoch_args_of(P, ej, B.optimiser, B.error, A);
                 sargs[warp] = A;
             }
             __syncwarp();
@@ -139,7 +142,7 @@ __global__ void __launch_bounds__(kWarps * 32, 8) k_batch_epoch(const BatchArgs 
     if (ej >= P.n_epochs) return;
     if (lane == 0) {
         EpochArgs A{};
-        epoch_args_of(P, ej, B.optimiser, A);
+        epoch_args_of(P, ej, B.optimiser, B.error, A);
         sargs[warp] = A;
     }
     __syncwarp();

@@ -65,6 +65,24 @@ __device__ __forceinline__ uint32_t range32(uint32_t x, uint32_t n) { return __u
 
 // ------------------------------------------------------------ helpers
 
+// Checked builds (compiled with UMAPCU_CHECKED): an index that would take an
+// access outside its array -- a CSR offset past the entries or out of order,
+// an other endpoint, injected negative or list record beyond the nodes -- is
+// reported (the error word becomes UMAPCU_BAD_ARG unless it already holds a
+// status) and the access is skipped, never performed. Other builds compile
+// every check away: checked_ok() is then the constant true.
+__device__ __forceinline__ bool checked_ok(bool ok, uint32_t *err)
+{
+#ifdef UMAPCU_CHECKED
+    if (!ok && err) atomicCAS(err, 0u, (uint32_t)UMAPCU_BAD_ARG);
+    return ok;
+#else
+    (void)ok;
+    (void)err;
+    return true;
+#endif
+}
+
 // L2 residency: the embedding (gathered at random every epoch) is loaded
 // with an evict_last policy; the CSR arrays (streamed once per epoch) with
 // the streaming (evict-first) qualifier, so they do not push the embedding
@@ -235,6 +253,7 @@ __device__ __forceinline__ unsigned process_batch(const EpochArgs &A, Smem &S, b
                                                   int lane, float (&g)[D], bool &act, const float *dstat,
                                                   float (*part)[D])
 {
+    if (live && !checked_ok(o < A.n && p < A.n_entries, A.err)) live = false;
     if (!live) j = 32;  // dead lanes: a node of their own, contributing zero
     float c[D];
 #pragma unroll
@@ -260,6 +279,7 @@ __device__ __forceinline__ unsigned process_batch(const EpochArgs &A, Smem &S, b
                 if (neg < neg_rate) {
                     if (!FAST && A.injected) {
                         kn = A.injected[(uint64_t)p * neg_rate + neg];
+                        if (!checked_ok(kn < A.n, A.err)) kn = self;  // skipped like a self sample
                     } else if (!FAST && A.sampler == UMAPCU_NEG_PHILOX) {
                         if ((t & 3) == 0) ph = philox4x32_10(make_uint4(p, A.epoch, neg >> 2, 0x554D4150u), A.seed_lo,
                                                              A.seed_hi);
@@ -391,6 +411,19 @@ __device__ __forceinline__ void load_segment(const EpochArgs &A, Smem &S, uint32
     if constexpr (DENS) {
         if (valid) S.dn[lane] = __ldg(A.dens_node + node);
     }
+#ifdef UMAPCU_CHECKED
+    // the segment's row starts must be in order and within the entries; a
+    // segment that breaks that is walked as empty
+    __syncwarp();
+    const bool bad = S.beg[lane + 1] < S.beg[lane] || S.beg[lane + 1] > A.n_entries;
+    if (__any_sync(kFull, bad)) {
+        if (lane == 0) checked_ok(false, A.err);
+        __syncwarp();
+        S.beg[lane] = 0;
+        if (lane == 31) S.beg[32] = 0;
+    }
+    __syncwarp();
+#endif
 }
 
 // The node's step (umap_adam_update, umap_optimiser_gpu.rs:887-923, or the
@@ -455,7 +488,10 @@ __device__ __forceinline__ void epoch_segment(const EpochArgs &A, WarpSmem<D, KU
         for (uint64_t q = r0; q < r1; q += 32) {
             const bool live = q + lane < r1;
             const uint32_t j = nx.x >> kRecNodeShift, el = nx.x & kRecOffsetMask, o = nx.y;
-            const uint32_t p = live ? S.beg[j] + el : 0u;  // unused (and not loaded) on the fast path
+            uint32_t p = live ? S.beg[j] + el : 0u;  // unused (and not loaded) on the fast path
+#ifdef UMAPCU_CHECKED
+            if (live && !checked_ok(p < S.beg[j + 1], A.err)) p = ~0u;  // refused in process_batch
+#endif
             if (q + 32 + lane < r1) nx = __ldcs(A.rec + q + 32 + lane);
             process_batch<D, DENS, NR, COH, KU, FAST>(A, S, live, p, o, j, el, node0, lane, g, act, dstat, S.part);
         }
@@ -619,7 +655,10 @@ __device__ __forceinline__ void epoch_segment_split(const EpochArgs &A, WarpSmem
         if (q < r1) {  // warp-uniform
             const bool live = q + lane < r1;
             const uint32_t j = nx.x >> kRecNodeShift, el = nx.x & kRecOffsetMask, o = nx.y;
-            const uint32_t p = live ? S.beg[j] + el : 0u;
+            uint32_t p = live ? S.beg[j] + el : 0u;
+#ifdef UMAPCU_CHECKED
+            if (live && !checked_ok(p < S.beg[j + 1], A.err)) p = ~0u;
+#endif
             if (q + stride + lane < r1) nx = __ldcs(A.rec + q + stride + lane);
             float gd[D];
             bool ad = false;
@@ -678,7 +717,10 @@ __device__ __forceinline__ void epoch_segment_split_bits(const EpochArgs &A, War
                                                          unsigned *has_w, uint32_t *wm, uint32_t *pre,
                                                          uint32_t node0, int warp, int lane)
 {
-    const uint32_t sbeg = A.offsets[node0], send = A.offsets[min(node0 + 32u, A.n)];
+    uint32_t sbeg = A.offsets[node0], send = A.offsets[min(node0 + 32u, A.n)];
+#ifdef UMAPCU_CHECKED
+    if (!checked_ok(sbeg <= send && send <= A.n_entries, A.err)) sbeg = send = 0;
+#endif
     const uint32_t w0 = sbeg >> 5, nw = send > sbeg ? ((send - 1) >> 5) - w0 + 1 : 0;
     if (nw > kSplitWords) {  // block-uniform
         if (warp == 0) epoch_segment<D, DENS, NR, false, kU, FAST, false, true>(A, S, node0, lane);

@@ -140,6 +140,18 @@ __global__ void __launch_bounds__(kDensBlock) k_dens_update(const DensArgs A)
 #pragma unroll
     for (int d = 0; d < D; d++) S.ys[lane][d] = ys[d];
     __syncwarp();
+#ifdef UMAPCU_CHECKED
+    {
+        const bool bad = S.beg[lane + 1] < S.beg[lane] || S.beg[lane + 1] > A.n_entries;
+        if (__any_sync(kFull, bad)) {
+            if (lane == 0) checked_ok(false, A.err);
+            __syncwarp();
+            S.beg[lane] = 0;
+            if (lane == 31) S.beg[32] = 0;
+        }
+        __syncwarp();
+    }
+#endif
     const uint32_t seg_beg = S.beg[0], seg_end = S.beg[32];
     const uint64_t pol = l2_keep_policy();
     float sum_sq = 0.0f, sum_phi = 0.0f;
@@ -151,16 +163,18 @@ __global__ void __launch_bounds__(kDensBlock) k_dens_update(const DensArgs A)
             const uint32_t p = c0 + 32u * u + lane;
             o[u] = p < seg_end ? __ldcs(A.other + p) : 0u;
         }
+        bool in_range[kDensU];
 #pragma unroll
         for (int u = 0; u < kDensU; u++) {
             const uint32_t p = c0 + 32u * u + lane;
-            if (p < seg_end) load_row_keep<D>(A.y, o[u], yo[u], pol);
+            in_range[u] = p < seg_end && checked_ok(o[u] < n, A.err);
+            if (in_range[u]) load_row_keep<D>(A.y, o[u], yo[u], pol);
         }
 #pragma unroll
         for (int u = 0; u < kDensU; u++) {
             if (c0 + 32u * u >= seg_end) break;  // warp-uniform
             const uint32_t p = c0 + 32u * u + lane;
-            const bool live = p < seg_end;
+            const bool live = in_range[u];
             uint32_t j = 32;
             float t[2] = {0.0f, 0.0f};
             if (live) {

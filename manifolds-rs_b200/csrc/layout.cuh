@@ -38,6 +38,8 @@ struct EpochArgs {
     uint64_t fastmod_M;
     uint32_t optimiser;
     bool precise_pow;          // CUDA powf instead of pow_pos
+    uint64_t n_entries;        // CSR entries (2E): the length of other / sched / mu_entry
+    uint32_t *err;             // checked builds: error word (UMAPCU_BAD_ARG on a bad index), or nullptr
 };
 
 // Arguments of one densMAP radius/statistics update.
@@ -54,6 +56,8 @@ struct DensArgs {
     float *stats;         // [5]
     float var_shift, lambda, mu_tot;
     bool precise_pow;
+    uint64_t n_entries;   // CSR entries: the length of other
+    uint32_t *err;        // checked builds: error word, or nullptr
 };
 
 inline uint64_t fastmod_magic(uint32_t n) { return n ? (~0ull / n) + 1 : 0; }

@@ -80,17 +80,20 @@ extern "C" umapcu_status umapcu_optimise_csr_noalloc(float *d_embd, uint32_t n, 
         const uint64_t nt = (uint64_t)n * n_dim;
         const size_t b_sched = round256(n_entries * sizeof(float2));
         const size_t b_vec = round256(nt * sizeof(float));
-        if (n_entries >= (1ull << 31) || b_sched + 3 * b_vec > kNoAllocScratchBytes) return UMAPCU_CAPACITY;
+        // the last 256 bytes hold the checked build's error word
+        if (n_entries >= (1ull << 31) || b_sched + 3 * b_vec > kNoAllocScratchBytes - 256) return UMAPCU_CAPACITY;
         cudaStream_t s = (cudaStream_t)cuda_stream;
         unsigned char *base = (unsigned char *)scratch_address();
         float2 *sched = (float2 *)base;
         float *y_alt = (float *)(base + b_sched);
         float *m = (float *)(base + b_sched + b_vec);
         float *v = (float *)(base + b_sched + 2 * b_vec);
+        uint32_t *err = (uint32_t *)(base + kNoAllocScratchBytes - 256);
         // the array keeps the previous call's contents: start every state
         // buffer from its initial value
         check_cuda(cudaMemsetAsync(m, 0, nt * sizeof(float), s), "cudaMemsetAsync");
         check_cuda(cudaMemsetAsync(v, 0, nt * sizeof(float), s), "cudaMemsetAsync");
+        check_cuda(cudaMemsetAsync(err, 0, sizeof(uint32_t), s), "cudaMemsetAsync");
         k_noalloc_sched_init<<<ceil_div(n_entries, 256), 256, 0, s>>>(d_period, sched, n_entries);
         check_launch("k_noalloc_sched_init");
         float *y[2] = {d_embd, y_alt};
@@ -121,13 +124,23 @@ extern "C" umapcu_status umapcu_optimise_csr_noalloc(float *d_embd, uint32_t n, 
             A.seed_hi = (uint32_t)(seed >> 32);
             A.fastmod_M = fastmod_magic(n);
             A.optimiser = UMAPCU_OPT_ADAM;
+            A.n_entries = n_entries;
+            A.err = err;
             launch_epoch(A, n_dim, false, s);
             cur ^= 1;
         }
         if (cur != 0)
             check_cuda(cudaMemcpyAsync(d_embd, y_alt, nt * sizeof(float), cudaMemcpyDeviceToDevice, s),
                        "cudaMemcpyAsync");
+#ifdef UMAPCU_CHECKED
+        // the checked build waits for the epochs to report their indices
+        uint32_t h = 0;
+        check_cuda(cudaMemcpyAsync(&h, err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+        check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+        return (umapcu_status)h;
+#else
         return UMAPCU_OK;
+#endif
     } catch (const Error &e) {
         return e.status;
     } catch (...) {

@@ -25,6 +25,16 @@ def test_library_exports_every_declared_symbol():
     assert not missing, missing
 
 
+def test_checked_library_exports_the_same_symbols():
+    import umapcu
+    path = os.path.join(os.path.dirname(umapcu.LIB_PATH), "libumapcu_checked.so")
+    lib = C.CDLL(path)
+    missing = [n for n in _declared("umapcu.h") if not hasattr(lib, n)]
+    assert not missing, missing
+    lib.umapcu_version.restype = C.c_char_p
+    assert b"checked" in lib.umapcu_version()
+
+
 def test_status_strings_and_version():
     import umapcu
     assert umapcu.version().startswith("umapcu")
