@@ -294,6 +294,27 @@ umapcu_status umapcu_server_submit(umapcu_server *sv, uint32_t n, uint32_t n_dim
                                    const umapcu_optim_params *params, uint64_t seed, uint32_t sampler,
                                    uint64_t *ticket);
 
+/* Checkpoint of a job (no counterpart in the reference, which keeps a
+ * layout's state only for the duration of one call,
+ * umap_optimiser_gpu.rs:278-348): copies the job's current embedding (and,
+ * when m / v are not NULL, its Adam moments) [n * n_dim] and the number of
+ * epochs it has run. A running job is read between two ticks (the call waits
+ * for the next tick boundary; the job keeps running); a job not admitted yet
+ * returns the state it was submitted with. UMAPCU_BAD_ARG for a finished,
+ * failed or unknown job, or one with a snapshot already in progress. */
+umapcu_status umapcu_server_snapshot(umapcu_server *sv, uint64_t ticket, float *embd, float *m, float *v,
+                                     uint32_t *epochs_done);
+
+/* Queues a job that resumes from a snapshot: the arguments of the job's
+ * umapcu_server_submit (same graph, parameters, seed and sampler) plus its
+ * snapshot's embedding, moments and epoch count (< params->n_epochs). The
+ * job runs epochs [epochs_done, n_epochs), its schedule cursors re-derived
+ * from the edge periods, and its result equals the uninterrupted job's. */
+umapcu_status umapcu_server_submit_resume(umapcu_server *sv, uint32_t n, uint32_t n_dim, const float *embd,
+                                          const uint64_t *adj_ptr, const uint32_t *adj_col, const float *adj_w,
+                                          const umapcu_optim_params *params, uint64_t seed, uint32_t sampler,
+                                          const float *m, const float *v, uint32_t epochs_done, uint64_t *ticket);
+
 /* *state: 0 pending, 1 running, 2 done, 3 failed or cancelled. */
 umapcu_status umapcu_server_poll(umapcu_server *sv, uint64_t ticket, int *state);
 

@@ -253,6 +253,9 @@ void launch_schedule_bits(const float2 *sched, uint64_t n_entries, uint32_t n_ep
 // Writes into csr.sched the cursors after `epochs` epochs from the reset
 // schedule (the state the per-epoch scan would have left).
 void materialise_schedule(DeviceCsr &csr, uint32_t epochs, cudaStream_t s);
+// The same for the `count` entries from offsets[node_lo] on (one job's rows
+// of a multi-graph CSR).
+void materialise_schedule_range(DeviceCsr &csr, uint32_t node_lo, uint64_t count, uint32_t epochs, cudaStream_t s);
 
 // Resets every entry's schedule cursor to its period (upload state,
 // umap_optimiser_gpu.rs:425-430).

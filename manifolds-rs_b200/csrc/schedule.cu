@@ -180,6 +180,21 @@ __global__ void k_sched_materialise(float2 *__restrict__ sched, uint64_t n_entri
     sched[p].x = c;
 }
 
+// Cursors of the entries [offsets[node_lo], offsets[node_lo] + count) after
+// `epochs` epochs from the reset schedule.
+__global__ void k_sched_materialise_range(const uint32_t *__restrict__ offsets, uint32_t node_lo, uint64_t count,
+                                          float2 *__restrict__ sched, uint32_t epochs)
+{
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    const uint64_t p = offsets[node_lo] + t;
+    const float per = sched[p].y;
+    float c = per;
+    for (uint32_t e = 0; e < epochs; e++)
+        if (c <= (float)e) c = c + per;
+    sched[p].x = c;
+}
+
 }  // namespace
 
 bool build_schedule_lists(const DeviceCsr &csr, uint32_t n_epochs, ScheduleLists &out, cudaStream_t s)
@@ -358,6 +373,13 @@ bool build_schedule_bits(const DeviceCsr &csr, uint32_t n_epochs, ScheduleBits &
     out.words = words;
     out.n_epochs = n_epochs;
     return true;
+}
+
+void materialise_schedule_range(DeviceCsr &csr, uint32_t node_lo, uint64_t count, uint32_t epochs, cudaStream_t s)
+{
+    if (!count) return;
+    k_sched_materialise_range<<<ceil_div(count, 256), 256, 0, s>>>(csr.offsets.p, node_lo, count, csr.sched.p, epochs);
+    check_launch("k_sched_materialise_range");
 }
 
 void materialise_schedule(DeviceCsr &csr, uint32_t epochs, cudaStream_t s)

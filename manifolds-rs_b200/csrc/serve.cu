@@ -27,6 +27,7 @@
 // the same alone and in any mix. Failures are reported per job (allocation,
 // a graph without edges, device error, bounded-wait timeout); cancellation
 // works on pending jobs.
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <deque>
@@ -72,6 +73,18 @@ struct ServeJob {
     uint32_t node_base = 0;       // first node of the job in the group's CSR
     uint64_t y_off = 0, sc_off = 0, n_edges = 0;
     uint32_t epochs_done = 0;
+    // a resumed job: epochs run before it was submitted, and its Adam moments
+    // in the submit block (o_m = 0: the moments start at zero)
+    uint32_t start_epoch = 0;
+    size_t o_m = 0, o_v = 0;
+    // a snapshot request, answered by the tick thread between two ticks
+    struct Snapshot {
+        float *y = nullptr, *m = nullptr, *v = nullptr;
+        uint32_t epochs = 0;
+        umapcu_status rc = UMAPCU_OK;
+        bool done = false;
+    };
+    Snapshot *snap = nullptr;
     std::vector<float> result;
     int state = kPending;
     umapcu_status rc = UMAPCU_OK;
@@ -220,7 +233,52 @@ struct umapcu_server {
     void free_block(ServeJob *j);
     void tick_launch();
     umapcu_status tick_finish();
+    void answer_snapshots(const std::vector<ServeJob *> &done);
+    void release_snapshot(ServeJob *j, umapcu_status rc);  // caller holds mu
 };
+
+// Ends a job's snapshot request with `rc`. Caller holds mu.
+void umapcu_server::release_snapshot(ServeJob *j, umapcu_status rc)
+{
+    if (!j->snap) return;
+    j->snap->rc = rc;
+    j->snap->done = true;
+    j->snap = nullptr;
+    cv_done.notify_all();
+}
+
+// Between two ticks (tick thread, nothing in flight on s): copies the state
+// of every running job with a snapshot request -- the embedding buffer its
+// next epoch reads, its moments, its epoch count -- to the requester; jobs
+// that finished in the last tick answer UMAPCU_BAD_ARG (nothing left to
+// resume).
+void umapcu_server::answer_snapshots(const std::vector<ServeJob *> &done)
+{
+    std::vector<ServeJob *> req;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        for (ServeJob *j : done) release_snapshot(j, UMAPCU_BAD_ARG);
+        for (ServeJob *j : active)
+            if (j->snap) req.push_back(j);
+    }
+    for (ServeJob *j : req) {
+        umapcu_status rc = UMAPCU_OK;
+        try {
+            const uint64_t nt = (uint64_t)j->n * j->n_dim;
+            const AdmitGroup &G = *j->grp;
+            const float *y = ((j->epochs_done & 1) ? G.y1.p : G.y0.p) + j->y_off;
+            d2h(j->snap->y, y, nt, s);
+            if (j->snap->m) d2h(j->snap->m, G.m.p + j->y_off, nt, s);
+            if (j->snap->v) d2h(j->snap->v, G.v.p + j->y_off, nt, s);
+            sync(s);
+        } catch (const Error &e) {
+            rc = e.status;
+        }
+        std::lock_guard<std::mutex> lk(mu);
+        j->snap->epochs = j->epochs_done;
+        release_snapshot(j, rc);
+    }
+}
 
 // Moves a group of pending jobs to the device (per job, straight from its
 // submit block), builds their graphs in one multi-graph build and their state
@@ -278,8 +336,9 @@ void umapcu_server::admit_group(std::vector<ServeJob *> &g, int k)
                 check_cuda(cudaMemcpyAsync(d.p + d_w + 4 * e, j->blk + j->o_w, 4 * j->nnz, cudaMemcpyHostToDevice, s),
                            "h2d");
             }
-            check_cuda(cudaMemcpyAsync(grp->y0.p + j->y_off, j->blk + j->o_y, 4 * nt, cudaMemcpyHostToDevice, s),
-                       "h2d");
+            // the buffer an epoch of this parity reads (a resumed job starts mid-run)
+            float *y_start = ((j->start_epoch & 1) ? grp->y1.p : grp->y0.p) + j->y_off;
+            check_cuda(cudaMemcpyAsync(y_start, j->blk + j->o_y, 4 * nt, cudaMemcpyHostToDevice, s), "h2d");
             check_cuda(cudaMemcpyAsync(grp->scal.p + j->sc_off, j->blk + j->o_sc, 16ull * j->params.n_epochs,
                                        cudaMemcpyHostToDevice, s), "h2d");
             e += j->nnz;
@@ -292,6 +351,19 @@ void umapcu_server::admit_group(std::vector<ServeJob *> &g, int k)
     }
     check_cuda(cudaMemsetAsync(grp->m.p, 0, 4 * y_tot, s), "memset");
     check_cuda(cudaMemsetAsync(grp->v.p, 0, 4 * y_tot, s), "memset");
+    for (uint32_t t = 0; t < J; t++) {
+        const ServeJob *j = g[t];
+        if (!j->start_epoch && !j->o_m) continue;
+        // a resumed job: its moments, and its cursors as the schedule left
+        // them after its first start_epoch epochs
+        const uint64_t nt = (uint64_t)j->n * j->n_dim;
+        if (j->o_m) {
+            check_cuda(cudaMemcpyAsync(grp->m.p + j->y_off, j->blk + j->o_m, 4 * nt, cudaMemcpyHostToDevice, s), "h2d");
+            check_cuda(cudaMemcpyAsync(grp->v.p + j->y_off, j->blk + j->o_v, 4 * nt, cudaMemcpyHostToDevice, s), "h2d");
+        }
+        if (j->start_epoch && edges[t])
+            materialise_schedule_range(grp->csr, j->node_base, 2 * edges[t], j->start_epoch, s);
+    }
     sync(s);  // the submit blocks and the header staging are free after this
     const double tc = now();
     std::lock_guard<std::mutex> lk(mu);
@@ -464,6 +536,7 @@ void umapcu_server::admit_loop(int k)
             }
             j->state = kFailed;
             j->t_done = t;
+            release_snapshot(j, j->rc);
             group_job_done(j);
             live--;
         }
@@ -503,6 +576,7 @@ void umapcu_server::finish_loop()
         group_job_done(j);
         j->t_done = now();
         j->state = j->rc == UMAPCU_OK ? kDone : kFailed;
+        release_snapshot(j, UMAPCU_BAD_ARG);  // asked for after its last tick
         live--;
         completed++;
         cv_done.notify_all();
@@ -550,6 +624,7 @@ void umapcu_server::loop()
             done.push_back(j);
         }
         active.swap(still);
+        answer_snapshots(done);
         std::lock_guard<std::mutex> lk(mu);
         for (ServeJob *j : done) finishing.push_back(j);
         if (!done.empty()) cv_fin.notify_all();
@@ -561,6 +636,7 @@ void umapcu_server::loop()
         for (ServeJob *j : *v) {
             j->rc = UMAPCU_CANCELLED;
             j->state = kFailed;
+            release_snapshot(j, UMAPCU_CANCELLED);
         }
     for (ServeJob *j : pending) {
         j->rc = UMAPCU_CANCELLED;
@@ -609,15 +685,21 @@ umapcu_status umapcu_server_create(uint64_t device_budget_bytes, uint32_t max_jo
     }
 }
 
-umapcu_status umapcu_server_submit(umapcu_server *sv, uint32_t n, uint32_t n_dim, const float *embd,
-                                   const uint64_t *adj_ptr, const uint32_t *adj_col, const float *adj_w,
-                                   const umapcu_optim_params *params, uint64_t seed, uint32_t sampler,
-                                   uint64_t *ticket)
+}  // extern "C"
+
+namespace {
+
+// Submit of a new job (m = v = nullptr, start_epoch = 0) or of a resumed one.
+umapcu_status submit_job(umapcu_server *sv, uint32_t n, uint32_t n_dim, const float *embd, const uint64_t *adj_ptr,
+                         const uint32_t *adj_col, const float *adj_w, const umapcu_optim_params *params,
+                         uint64_t seed, uint32_t sampler, const float *m, const float *v, uint32_t start_epoch,
+                         uint64_t *ticket)
 {
     if (!sv || !ticket) return UMAPCU_BAD_ARG;
     if (n == 0) return UMAPCU_NO_DATA;
     if (!embd || !adj_ptr || !params || n_dim != sv->n_dim || params->n_epochs == 0 || sampler > UMAPCU_NEG_PHILOX)
         return UMAPCU_BAD_ARG;
+    if (start_epoch >= params->n_epochs || (!m) != (!v)) return UMAPCU_BAD_ARG;
     const uint64_t nnz = adj_ptr[n];
     if (nnz && (!adj_col || !adj_w)) return UMAPCU_BAD_ARG;
     if (adj_ptr[0] != 0) return UMAPCU_BAD_ARG;
@@ -638,6 +720,13 @@ umapcu_status umapcu_server_submit(umapcu_server *sv, uint32_t n, uint32_t n_dim
     j->o_y = j->o_w + align256(4 * nnz);
     j->o_sc = j->o_y + align256(4 * nt);
     j->blk_bytes = j->o_sc + 16ull * params->n_epochs;
+    j->start_epoch = start_epoch;
+    j->epochs_done = start_epoch;
+    if (m) {
+        j->o_m = align256(j->blk_bytes);
+        j->o_v = j->o_m + align256(4 * nt);
+        j->blk_bytes = j->o_v + 4 * nt;
+    }
     j->blk = sv->arena.alloc(j->blk_bytes, &j->chunk);
     if (!j->blk) {
         j->heap.resize(j->blk_bytes);
@@ -657,6 +746,10 @@ umapcu_status umapcu_server_submit(umapcu_server *sv, uint32_t n, uint32_t n_dim
     }
     memcpy(j->blk + j->o_w, adj_w, 4 * nnz);
     memcpy(j->blk + j->o_y, embd, 4 * nt);
+    if (m) {
+        memcpy(j->blk + j->o_m, m, 4 * nt);
+        memcpy(j->blk + j->o_v, v, 4 * nt);
+    }
     float4 *sc = (float4 *)(j->blk + j->o_sc);
     for (uint32_t e = 0; e < params->n_epochs; e++) {
         float f, ep, lr;
@@ -675,6 +768,59 @@ umapcu_status umapcu_server_submit(umapcu_server *sv, uint32_t n, uint32_t n_dim
     sv->jobs[j->id] = std::move(j);
     sv->cv_admit.notify_all();
     return UMAPCU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+umapcu_status umapcu_server_submit(umapcu_server *sv, uint32_t n, uint32_t n_dim, const float *embd,
+                                   const uint64_t *adj_ptr, const uint32_t *adj_col, const float *adj_w,
+                                   const umapcu_optim_params *params, uint64_t seed, uint32_t sampler,
+                                   uint64_t *ticket)
+{
+    return submit_job(sv, n, n_dim, embd, adj_ptr, adj_col, adj_w, params, seed, sampler, nullptr, nullptr, 0,
+                      ticket);
+}
+
+umapcu_status umapcu_server_submit_resume(umapcu_server *sv, uint32_t n, uint32_t n_dim, const float *embd,
+                                          const uint64_t *adj_ptr, const uint32_t *adj_col, const float *adj_w,
+                                          const umapcu_optim_params *params, uint64_t seed, uint32_t sampler,
+                                          const float *m, const float *v, uint32_t epochs_done, uint64_t *ticket)
+{
+    if (!m || !v) return UMAPCU_BAD_ARG;
+    return submit_job(sv, n, n_dim, embd, adj_ptr, adj_col, adj_w, params, seed, sampler, m, v, epochs_done,
+                      ticket);
+}
+
+umapcu_status umapcu_server_snapshot(umapcu_server *sv, uint64_t ticket, float *embd, float *m, float *v,
+                                     uint32_t *epochs_done)
+{
+    if (!sv || !embd || !epochs_done) return UMAPCU_BAD_ARG;
+    std::unique_lock<std::mutex> lk(sv->mu);
+    auto it = sv->jobs.find(ticket);
+    if (it == sv->jobs.end()) return UMAPCU_BAD_ARG;
+    ServeJob *j = it->second.get();
+    if (j->state == kDone || j->state == kFailed || j->snap) return UMAPCU_BAD_ARG;
+    const uint64_t nt = (uint64_t)j->n * j->n_dim;
+    if (std::find(sv->pending.begin(), sv->pending.end(), j) != sv->pending.end()) {
+        // not admitted yet: the state it was submitted with (admission cannot
+        // take it from the queue while the lock is held)
+        memcpy(embd, j->blk + j->o_y, 4 * nt);
+        if (m) j->o_m ? (void)memcpy(m, j->blk + j->o_m, 4 * nt) : (void)memset(m, 0, 4 * nt);
+        if (v) j->o_v ? (void)memcpy(v, j->blk + j->o_v, 4 * nt) : (void)memset(v, 0, 4 * nt);
+        *epochs_done = j->start_epoch;
+        return UMAPCU_OK;
+    }
+    ServeJob::Snapshot req;
+    req.y = embd;
+    req.m = m;
+    req.v = v;
+    j->snap = &req;
+    sv->cv_work.notify_all();
+    sv->cv_done.wait(lk, [&] { return req.done; });
+    *epochs_done = req.epochs;
+    return req.rc;
 }
 
 umapcu_status umapcu_server_poll(umapcu_server *sv, uint64_t ticket, int *state)
@@ -757,7 +903,9 @@ void umapcu_server_destroy(umapcu_server *sv)
         for (ServeJob *j : sv->ready) {
             j->rc = UMAPCU_CANCELLED;
             j->state = kFailed;
+            sv->release_snapshot(j, UMAPCU_CANCELLED);
         }
+        for (auto &kv : sv->jobs) sv->release_snapshot(kv.second.get(), UMAPCU_CANCELLED);
         sv->ready.clear();
         sv->cv_done.notify_all();
         if (getenv("UMAPCU_TIMING"))

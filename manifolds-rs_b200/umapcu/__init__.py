@@ -161,6 +161,8 @@ _SIGS = {
     "umapcu_probe_l2_gather": [_u64, _vp],
     "umapcu_device_count": [_vp],
     "umapcu_server_job_bytes": [_u32, _u32, _u64, _u32, _vp],
+    "umapcu_server_snapshot": [_vp, _u64, _vp, _vp, _vp, _vp],
+    "umapcu_server_submit_resume": [_vp, _u32, _u32, _vp, _vp, _vp, _vp, _vp, _u64, _u32, _vp, _vp, _u32, _vp],
     "umapcu_set_device": [_i32],
 }
 for _name, _args in _SIGS.items():
@@ -604,6 +606,37 @@ class UmapServer:
                                          _p(a.w), C.byref(cp), int(seed) & (2 ** 64 - 1), sampler, C.byref(t)))
         self._n[t.value] = e.shape[0]
         return t.value
+
+    def submit_resume(self, embd, graph, params: UmapOptimParams, m, v, epochs_done: int, seed: int = 42,
+                      sampler: int = NEG_REF_HASH) -> int:
+        """Queues a job resuming from a snapshot (embedding, moments, epochs
+        run) of a job with the same graph, parameters, seed and sampler; its
+        result equals the uninterrupted job's."""
+        e = _c(embd, np.float32)
+        mm, vv = _c(m, np.float32), _c(v, np.float32)
+        if mm.shape != e.shape or vv.shape != e.shape:
+            raise ManifoldsError(BAD_ARG, "m and v must have the embedding's shape")
+        a = _adj(graph)
+        cp = params._c()
+        t = C.c_uint64()
+        _check(_lib.umapcu_server_submit_resume(self._h, e.shape[0], e.shape[1], _p(e), _p(_c(a.ptr, np.uint64)),
+                                                _p(a.col), _p(a.w), C.byref(cp), int(seed) & (2 ** 64 - 1), sampler,
+                                                _p(mm), _p(vv), int(epochs_done), C.byref(t)))
+        self._n[t.value] = e.shape[0]
+        return t.value
+
+    def snapshot(self, ticket: int):
+        """-> (embedding, m, v, epochs_done) of a pending or running job (a
+        running one is read at the next tick boundary and keeps running)."""
+        n = self._n.get(ticket)
+        if n is None:
+            raise ManifoldsError(BAD_ARG, "unknown ticket")
+        y = np.empty((n, self.n_dim), np.float32)
+        m = np.empty_like(y)
+        v = np.empty_like(y)
+        ep = C.c_uint32()
+        _check(_lib.umapcu_server_snapshot(self._h, ticket, _p(y), _p(m), _p(v), C.byref(ep)), "snapshot")
+        return y, m, v, ep.value
 
     def poll(self, ticket: int) -> int:
         st = C.c_int()

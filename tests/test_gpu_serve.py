@@ -136,3 +136,31 @@ def test_submit_rejects_malformed_graphs(pool):
     y, _, _ = sv.wait(sv.submit(init, adj, P60, seed=21))  # the server is unaffected
     assert np.array_equal(y, _alone(adj, init, 21))
     sv.close()
+
+
+def test_snapshot_and_resume_equal_the_uninterrupted_job(pool):
+    """A running job's snapshot (embedding, Adam moments, epochs run, read at
+    a tick boundary) resumed as a new job gives the uninterrupted job's
+    result bit for bit; a job not admitted yet snapshots to the state it was
+    submitted with."""
+    adj, init = pool[3]
+    p = umapcu.UmapOptimParams(n_epochs=3000)
+    sv = umapcu.UmapServer(budget_bytes=8 << 30, max_jobs=1, tick_epochs=7)
+    ta = sv.submit(init, adj, p, seed=77)
+    tb = sv.submit(pool[1][1], pool[1][0], P60, seed=5)  # queued behind ta (one job at a time)
+    yb, mb, vb, eb = sv.snapshot(tb)
+    assert eb == 0 and np.array_equal(yb, pool[1][1]) and not mb.any() and not vb.any()
+    t0 = time.time()
+    while sv.poll(ta) != umapcu.UmapServer.RUNNING and time.time() - t0 < 30:
+        time.sleep(0.001)
+    y, m, v, e = sv.snapshot(ta)
+    assert 0 < e < 3000 and e % 7 == 0 and np.isfinite(y).all() and m.any()
+    tc = sv.submit_resume(y, adj, p, m, v, e, seed=77)
+    ya = sv.wait(ta)[0]
+    sv.wait(tb)
+    yc = sv.wait(tc)[0]
+    assert np.array_equal(yc, ya)
+    assert np.array_equal(ya, _alone(adj, init, 77, p))
+    with pytest.raises(umapcu.ManifoldsError):
+        sv.snapshot(ta)  # collected: unknown ticket
+    sv.close()
