@@ -367,7 +367,10 @@ def main():
     ae = active_edges_per_epoch(csr["eps"], wl["n_epochs"])
     updates_per_step = int(ae.sum())
     n_ep = wl["n_epochs"]
-    stream = torch.cuda.current_stream()
+    # a stream of our own (the legacy default stream's handle is 0, which the
+    # state reads as "your own stream"): the state's launches and the events
+    # share it
+    stream = torch.cuda.Stream()
     st.set_stream(stream.cuda_stream)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > L2
 
@@ -618,7 +621,7 @@ def run_batched(args, wl, world, rank, local_rank):
         updates += int(active_edges_per_epoch(st.csr()["eps"], wl["n_epochs"]).sum())
         states.append(st)
     # sequential plain-kernel runs of the same problems (device-resident states)
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream()
     for st in states:
         st.set_stream(stream.cuda_stream)
     for i, st in enumerate(states[:8]):
@@ -631,7 +634,7 @@ def run_batched(args, wl, world, rank, local_rank):
     torch.cuda.synchronize()
     e0.record(stream)
     for st in states:
-        st.run(0, wl["n_epochs"])
+        st.enqueue(0, wl["n_epochs"])
     e1.record(stream)
     torch.cuda.synchronize()
     t_seq = max_over_ranks(e0.elapsed_time(e1) / 1e3, group)

@@ -835,10 +835,11 @@ def knn_exact(data: np.ndarray, k: int, dist_metric="euclidean"):
 
 
 def embedding_quality(data: np.ndarray, embd: np.ndarray, knn_idx=None, k: int = 15, queries=None,
-                      dist_metric="euclidean"):
+                      dist_metric="euclidean", trust: bool = True):
     """trustworthiness@k (sklearn's definition) and kNN preservation@k of an
     embedding, on the GPU, over the query rows (all rows by default).
-    -> dict(trust=..., knn_preservation=... or None)."""
+    trust=False skips trustworthiness (the ranks in the data space, the
+    expensive part). -> dict(trust=... or None, knn_preservation=... or None)."""
     X = _c(data, np.float32)
     Y = _c(embd, np.float32)
     n = X.shape[0]
@@ -848,9 +849,10 @@ def embedding_quality(data: np.ndarray, embd: np.ndarray, knn_idx=None, k: int =
     kp = C.c_double()
     _check(_lib.umapcu_embedding_quality(_p(X), n, X.shape[1], _p(Y), Y.shape[1], _p(ki),
                                          0 if ki is None else ki.shape[1], k, _p(q), 0 if q is None else q.size,
-                                         _metric(dist_metric), C.byref(t), None if ki is None else C.byref(kp)),
+                                         _metric(dist_metric), C.byref(t) if trust else None,
+                                         None if ki is None else C.byref(kp)),
            "embedding_quality")
-    return dict(trust=t.value, knn_preservation=None if ki is None else kp.value)
+    return dict(trust=t.value if trust else None, knn_preservation=None if ki is None else kp.value)
 
 
 def fuzzy_cross_entropy(graph: "CoordinateList", embd: np.ndarray, a: float, b: float) -> float:

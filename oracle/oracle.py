@@ -43,6 +43,8 @@ def lib():
         build()
         L = C.CDLL(_LIB_PATH)
         vp = C.c_void_p
+        L.orc_set_exp_mode.argtypes = [C.c_int]
+        L.orc_set_exp_mode.restype = None
         L.orc_local_connectivity_distance.restype = C.c_float
         L.orc_local_connectivity_distance.argtypes = [f32p, C.c_uint32, C.c_float]
         L.orc_smooth_knn_dist.argtypes = [f32p, C.c_uint32, C.c_uint32, C.c_float, C.c_float,
@@ -126,6 +128,15 @@ def _ptr(a):
 
 
 # ---------------------------------------------------------------- graph
+
+EXP_GLIBC, EXP_FROM_DOUBLE = 0, 1
+
+
+def set_exp_mode(mode):
+    """The graph stage's exp: EXP_GLIBC (glibc expf, the reference's; the
+    default) or EXP_FROM_DOUBLE ((float)exp((double)x), the device's form),
+    for attributing a difference to the last bit of expf."""
+    lib().orc_set_exp_mode(int(mode))
 
 def local_connectivity_distance(dists, local_connectivity):
     d = _f32(dists)

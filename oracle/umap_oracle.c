@@ -64,6 +64,18 @@ float orc_local_connectivity_distance(const float *dists, uint32_t k, float lc)
     return dists[idx];
 }
 
+/* The exp of the graph stage (smooth_knn_dist, knn_to_coo). 0 (default):
+ * glibc's expf, what the reference's f32::exp calls. 1: exp rounded from
+ * double, (float)exp((double)x) -- the device's form; a test switches to it
+ * only to attribute a difference from the device to the last bit of expf
+ * (glibc's expf and the correctly rounded exp differ for about 0.06 % of
+ * arguments). */
+static int orc_exp_mode = 0;
+
+void orc_set_exp_mode(int mode) { orc_exp_mode = mode; }
+
+static inline float orc_graph_exp(float x) { return orc_exp_mode ? (float)exp((double)x) : expf(x); }
+
 /* graph.rs:499-565 smooth_knn_dist. Row length k is the reference's `k`
  * argument (lib.rs:298 passes knn_dist[0].len()). */
 void orc_smooth_knn_dist(const float *dist, uint32_t n, uint32_t k, float local_connectivity,
@@ -83,7 +95,7 @@ void orc_smooth_knn_dist(const float *dist, uint32_t n, uint32_t k, float local_
             for (uint32_t it = 0; it < n_iter; it++) {
                 float inv_mid = 1.0f / mid;
                 float s = -0.0f; /* Rust's f32 Sum folds from -0.0 */
-                for (uint32_t t = 0; t < k; t++) s += expf((-adjusted[t]) * inv_mid);
+                for (uint32_t t = 0; t < k; t++) s += orc_graph_exp((-adjusted[t]) * inv_mid);
                 double val = (double)s;
                 if (fabs(val - target) < tol) break;
                 if (val > target) {
@@ -118,7 +130,7 @@ uint64_t orc_knn_to_coo(const int32_t *knn_idx, const float *knn_dist, uint32_t 
             if ((uint32_t)j == i) continue;
             float adjusted = fmaxf(knn_dist[(uint64_t)i * k + t] - rho, 0.0f);
             float weight;
-            if (smooth) weight = expf((-adjusted) * inv_sigma);
+            if (smooth) weight = orc_graph_exp((-adjusted) * inv_sigma);
             else if (adjusted > 0.0f) weight = 0.0f;
             else weight = 1.0f;
             row[w] = i;

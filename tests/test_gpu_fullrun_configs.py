@@ -15,12 +15,13 @@ so that their standard errors sit well below 1 %:
   side, every metric over all points;
 * C3, 200k x 30, 20 clusters of different spread, k = 30, 200 epochs with
   the densMAP term in the last 30 %: 8 seeds per side;
-* C2, 1M x 50, 30 anisotropic components, k = 15, 200 epochs: one oracle run
-  (tens of seconds on the host cores) against the mean of 4 GPU runs.
+* C2, 1M x 50, 30 anisotropic components, k = 15, 200 epochs: 3 oracle runs
+  (each some ten seconds on the host cores) against 4 GPU runs.
 
-trust and kNN preservation on C2 and C3 are evaluated on a seeded 10 000-query
-subsample against all points, the same queries on both sides. The measured
-means, spreads and differences are printed (pytest -s) for the record.
+trust on C2 and C3 is evaluated on a seeded 10 000-query subsample against
+all points (the same queries on both sides), kNN preservation and the
+cross-entropy over every point and edge. The measured means, spreads and
+differences are printed (pytest -s) for the record.
 """
 import multiprocessing as mp
 import os
@@ -63,9 +64,15 @@ def _oracle_runs(g, init, p, seeds, dens, procs):
 
 
 def _metrics(g, Y, p, queries):
-    q = umapcu.embedding_quality(g["X"], Y, g["idx"].astype(np.int32)[:, :15], 15, queries=queries)
+    """trust@15 over the queries; kNN preservation@15 over every point (at
+    1M points it counts ~20k shared neighbours: on a 10 000-query subsample
+    it would rest on ~200 and carry several per cent of counting noise);
+    fuzzy cross-entropy over every graph edge."""
+    ki = g["idx"].astype(np.int32)[:, :15]
+    t = umapcu.embedding_quality(g["X"], Y, None, 15, queries=queries)["trust"]
+    kp = umapcu.embedding_quality(g["X"], Y, ki, 15, trust=False)["knn_preservation"]
     coo = umapcu.CoordinateList(g["row"], g["col"], g["val"], g["n"])
-    return np.array([q["trust"], q["knn_preservation"], umapcu.fuzzy_cross_entropy(coo, Y, p.a, p.b)])
+    return np.array([t, kp, umapcu.fuzzy_cross_entropy(coo, Y, p.a, p.b)])
 
 
 def _compare(name, mg, mo):
@@ -142,5 +149,5 @@ def test_full_run_quality_c2():
         umapcu.optimise_embedding_adam_gpu(y, adj, p, None, s)
         assert np.isfinite(y).all()
         mg.append(_metrics(g, y, p, qs))
-    yo = _oracle_runs(g, init, p, [0], None, 1)[0]
-    _compare("c2", mg, [_metrics(g, yo, p, qs)])
+    yos = _oracle_runs(g, init, p, [0, 1, 2], None, 1)
+    _compare("c2", mg, [_metrics(g, y, p, qs) for y in yos])
