@@ -173,27 +173,34 @@ inline void launch_batch_kernel_t(const BatchArgs &B, const BatchConfig &c, cuda
     check_launch("k_batch");
 }
 
-// bits: every problem carries its schedule bitmasks (the batched form; the
-// served form scans the cursors)
+// bits: every problem carries its schedule bitmasks (P.bits), scanned in
+// place of the cursors (the batched form with the fast kernels; the served
+// form always)
 template <int D>
 inline void launch_batch_kernel(const BatchArgs &B, const BatchConfig &c, cudaStream_t s, uint32_t epoch,
                                 bool fast, bool bits = false)
 {
     if (fast && bits) launch_batch_kernel_t<D, true, true>(B, c, s, epoch);
     else if (fast) launch_batch_kernel_t<D, true, false>(B, c, s, epoch);
+    else if (bits) launch_batch_kernel_t<D, false, true>(B, c, s, epoch);
     else launch_batch_kernel_t<D, false, false>(B, c, s, epoch);
 }
 
+// Problems with other negative sample rates (NR = 0: the rate is a runtime
+// value); bits as above.
 template <int D>
-inline void launch_batch_kernel_nr0(const BatchArgs &B, const BatchConfig &c, cudaStream_t s, uint32_t epoch)
+inline void launch_batch_kernel_nr0(const BatchArgs &B, const BatchConfig &c, cudaStream_t s, uint32_t epoch,
+                                    bool bits = false)
 {
     if (c.mode == 1) {
         const unsigned grid = (unsigned)(c.ctas_per_sm * device_sm_count());
-        if (c.ku == 4) k_batch_persistent<D, 0, 4><<<grid, kWarps * 32, 0, s>>>(B);
+        if (bits) k_batch_persistent<D, 0, 8, false, true><<<grid, kWarps * 32, 0, s>>>(B);
+        else if (c.ku == 4) k_batch_persistent<D, 0, 4><<<grid, kWarps * 32, 0, s>>>(B);
         else k_batch_persistent<D, 0, 8><<<grid, kWarps * 32, 0, s>>>(B);
     } else {
         const unsigned grid = ceil_div(B.n_segs, kWarps);
-        if (c.ku == 4) k_batch_epoch<D, 0, 4><<<grid, kWarps * 32, 0, s>>>(B, epoch);
+        if (bits) k_batch_epoch<D, 0, 8, false, true><<<grid, kWarps * 32, 0, s>>>(B, epoch);
+        else if (c.ku == 4) k_batch_epoch<D, 0, 4><<<grid, kWarps * 32, 0, s>>>(B, epoch);
         else k_batch_epoch<D, 0, 8><<<grid, kWarps * 32, 0, s>>>(B, epoch);
     }
     check_launch("k_batch");

@@ -51,6 +51,11 @@ struct AdmitGroup {
     DeviceCsr csr;                // all the group's nodes; each job uses its slice
     DevBuf<float> y0, y1, m, v;   // per-job slices, 256-byte aligned
     DevBuf<float4> scal;          // per-job epoch scalars
+    // the edge schedule of every CSR entry of the group, per epoch, as
+    // bitmasks [max n_epochs][bits_words] (bit p of an epoch: entry p active):
+    // the ticks scan these in place of the cursors
+    DevBuf<uint32_t> bits;
+    uint64_t bits_words = 0;
     uint64_t bytes = 0;           // admission estimate held against the budget
     uint32_t remaining = 0;       // jobs still running
 };
@@ -92,10 +97,11 @@ struct ServeJob {
 };
 
 // Peak device bytes of admitting and running a job: the CSR build's
-// temporaries dominate (about 64 B per adjacency entry), plus the state.
+// temporaries dominate (about 64 B per adjacency entry), plus the state and
+// the schedule bitmasks (one bit per CSR entry -- at most nnz -- and epoch).
 uint64_t job_bytes(uint32_t n, uint32_t n_dim, uint64_t nnz, uint32_t n_epochs)
 {
-    return 72ull * nnz + 24ull * n * n_dim + 16ull * n_epochs + (1ull << 20);
+    return 72ull * nnz + 24ull * n * n_dim + 16ull * n_epochs + (nnz + 32) / 8 * n_epochs + (1ull << 20);
 }
 
 }  // namespace
@@ -351,6 +357,18 @@ void umapcu_server::admit_group(std::vector<ServeJob *> &g, int k)
     }
     check_cuda(cudaMemsetAsync(grp->m.p, 0, 4 * y_tot, s), "memset");
     check_cuda(cudaMemsetAsync(grp->v.p, 0, 4 * y_tot, s), "memset");
+    {
+        // schedule bitmasks of the whole group (from the periods, so valid for
+        // resumed jobs too: they are indexed by the job's own epoch)
+        uint32_t max_ep = 0;
+        for (const ServeJob *j : g) max_ep = std::max(max_ep, j->params.n_epochs);
+        const uint64_t entries = 2 * grp->csr.n_edges;
+        grp->bits_words = (entries + 31) / 32;
+        if (entries) {
+            grp->bits.alloc((size_t)grp->bits_words * max_ep, s);
+            launch_schedule_bits(grp->csr.sched.p, entries, max_ep, grp->bits.p, s);
+        }
+    }
     for (uint32_t t = 0; t < J; t++) {
         const ServeJob *j = g[t];
         if (!j->start_epoch && !j->o_m) continue;
@@ -409,6 +427,7 @@ void umapcu_server::group_job_done(ServeJob *j)
     grp->m.release();
     grp->v.release();
     grp->scal.release();
+    grp->bits.release();
 }
 
 // Enqueues one tick over the active jobs on stream s (asynchronous).
@@ -435,6 +454,8 @@ void umapcu_server::tick_launch()
         P.m = G.m.p + j->y_off;
         P.v = G.v.p + j->y_off;
         P.scal = G.scal.p + j->sc_off;
+        P.bits = G.bits.p;
+        P.bits_words = G.bits_words;
         P.n_entries = 2 * j->n_edges;
         const umapcu_optim_params &q = j->params;
         P.a = q.a;
@@ -475,9 +496,9 @@ void umapcu_server::tick_launch()
     c.mode = 1;
     c.ctas_per_sm = tick_ctas;
     switch (n_dim) {
-        case 2: nr5 ? launch_batch_kernel<2>(B, c, s, 0, all_hash) : launch_batch_kernel_nr0<2>(B, c, s, 0); break;
-        case 3: nr5 ? launch_batch_kernel<3>(B, c, s, 0, all_hash) : launch_batch_kernel_nr0<3>(B, c, s, 0); break;
-        default: nr5 ? launch_batch_kernel<4>(B, c, s, 0, all_hash) : launch_batch_kernel_nr0<4>(B, c, s, 0); break;
+        case 2: nr5 ? launch_batch_kernel<2>(B, c, s, 0, all_hash, true) : launch_batch_kernel_nr0<2>(B, c, s, 0, true); break;
+        case 3: nr5 ? launch_batch_kernel<3>(B, c, s, 0, all_hash, true) : launch_batch_kernel_nr0<3>(B, c, s, 0, true); break;
+        default: nr5 ? launch_batch_kernel<4>(B, c, s, 0, all_hash, true) : launch_batch_kernel_nr0<4>(B, c, s, 0, true); break;
     }
     d2h(&err_h, ctr.p + 1, 1, s);
 }
