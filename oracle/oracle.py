@@ -77,6 +77,8 @@ def lib():
         L.orc_grad_accum.argtypes = [f32p, C.c_uint32, C.c_uint32, u32p, u32p, u32p, f32p, C.c_uint32,
                                      C.c_uint64, C.c_uint32, C.c_uint32, C.c_float, C.c_float, C.c_float,
                                      vp, vp, vp, vp, C.c_float, vp, f32p, vp]
+        L.orc_set_grad_abs_sum.argtypes = [C.c_void_p]
+        L.orc_set_grad_abs_sum.restype = None
         L.orc_adam_update.argtypes = [f32p, u32p, f32p, f32p, f32p, C.c_uint32, C.c_uint32, C.c_float,
                                       C.c_float, C.c_float, C.c_float]
         L.orc_schedule_update.argtypes = [f32p, f32p, C.c_uint64, C.c_uint32]
@@ -281,11 +283,13 @@ def dens_weights(r, re, var_shift, lam, mu_tot):
 
 
 def grad_accum(embd, csr, cursor, epoch, seed, neg_rate, a, b, gamma, sampler=SAMPLER_HASH,
-               dens=None, injected=None):
+               dens=None, injected=None, abs_sum=None):
     """umap_optimiser_gpu.rs:1461-1579 (+ has_update of :737-742, :859).
 
     dens: None or dict(re, phi_sum, weight, coeff). injected: None or
-    uint32 [2E, neg_rate] of negative nodes per CSR entry."""
+    uint32 [2E, neg_rate] of negative nodes per CSR entry. abs_sum: None or a
+    float64 [n, n_dim] array that receives the sum of |term| per node and
+    coordinate (the scale of the f32 sum's own rounding)."""
     e = _f32(embd)
     n, d = e.shape
     grad = np.zeros((n, d), np.float32)
@@ -299,9 +303,15 @@ def grad_accum(embd, csr, cursor, epoch, seed, neg_rate, a, b, gamma, sampler=SA
         re = phi = wt = mu = None
         coeff = 0.0
     inj = None if injected is None else np.ascontiguousarray(injected, dtype=np.uint32)
-    lib().orc_grad_accum(e, n, d, csr["offsets"], _u32(csr["edge_idx"]), _u32(csr["other"]), cur,
-                         epoch, seed, sampler, neg_rate, a, b, gamma, _ptr(mu), _ptr(re), _ptr(phi),
-                         _ptr(wt), coeff, _ptr(inj), grad, hu.ctypes.data_as(C.c_void_p))
+    if abs_sum is not None:
+        assert abs_sum.dtype == np.float64 and abs_sum.shape == (n, d) and abs_sum.flags.c_contiguous
+    lib().orc_set_grad_abs_sum(_ptr(abs_sum))
+    try:
+        lib().orc_grad_accum(e, n, d, csr["offsets"], _u32(csr["edge_idx"]), _u32(csr["other"]), cur,
+                             epoch, seed, sampler, neg_rate, a, b, gamma, _ptr(mu), _ptr(re), _ptr(phi),
+                             _ptr(wt), coeff, _ptr(inj), grad, hu.ctypes.data_as(C.c_void_p))
+    finally:
+        lib().orc_set_grad_abs_sum(None)
     return grad, hu
 
 

@@ -503,7 +503,14 @@ float orc_dens_weights(const float *r, const float *re, uint32_t n, float var_sh
 /* umap_optimiser_gpu.rs:1461-1579 cpu_grad_accum (== kernel :682-860), plus
  * the has_update flag the kernel writes (:737-742, :859). Cursor array is
  * per edge. Negative source: sampler (hash / philox) or, when inj != NULL,
- * inj[pos * neg_rate + neg] for CSR entry pos. dens_* may be NULL. */
+ * inj[pos * neg_rate + neg] for CSR entry pos. dens_* may be NULL.
+ * abs_sum (test aid, may be NULL): per node and coordinate, the sum of the
+ * absolute values of the terms added into the gradient, in f64 -- the scale
+ * of the f32 sum's own rounding (a few units of 2^-24 times it). */
+static double *orc_grad_abs_sum = NULL;
+
+void orc_set_grad_abs_sum(double *abs_sum) { orc_grad_abs_sum = abs_sum; }
+
 void orc_grad_accum(const float *embd, uint32_t n, uint32_t n_dim, const uint32_t *offsets,
                     const uint32_t *edge_idx, const uint32_t *other, const float *cursor,
                     uint32_t epoch, uint64_t seed, uint32_t sampler, uint32_t neg_rate, float a,
@@ -511,6 +518,7 @@ void orc_grad_accum(const float *embd, uint32_t n, uint32_t n_dim, const uint32_
                     const float *dens_phi_sum, const float *dens_weight, float dens_coeff,
                     const uint32_t *inj, float *grad, uint32_t *has_update)
 {
+    double *abs_sum = orc_grad_abs_sum;
     const float two = 2.0f, one = 1.0f;
     const float two_a_b = two * a * b;
     const float two_gamma_b = two * gamma * b;
@@ -518,11 +526,13 @@ void orc_grad_accum(const float *embd, uint32_t n, uint32_t n_dim, const uint32_
     const float epoch_t = (float)epoch;
     const uint32_t seed_u32 = (uint32_t)seed;
     float g[16];
-#pragma omp parallel for schedule(dynamic, 256) private(g)
+    double ga[16];
+#pragma omp parallel for schedule(dynamic, 256) private(g, ga)
     for (int64_t node_s = 0; node_s < (int64_t)n; node_s++) {
         uint32_t node = (uint32_t)node_s;
         uint64_t base_self = (uint64_t)node * n_dim;
         for (uint32_t d = 0; d < n_dim; d++) g[d] = 0.0f;
+        for (uint32_t d = 0; d < n_dim; d++) ga[d] = 0.0;
         uint32_t edge_local = 0, active = 0;
         for (uint32_t pos = offsets[node]; pos < offsets[node + 1]; pos++, edge_local++) {
             uint32_t e = edge_idx[pos];
@@ -542,6 +552,7 @@ void orc_grad_accum(const float *embd, uint32_t n, uint32_t n_dim, const uint32_
                 for (uint32_t d = 0; d < n_dim; d++) {
                     float delta = embd[base_other + d] - embd[base_self + d];
                     g[d] += two * grad_coeff * delta;
+                    ga[d] += fabs((double)(two * grad_coeff * delta));
                 }
                 if (dens_re) {
                     float phi = one / denom;
@@ -557,6 +568,7 @@ void orc_grad_accum(const float *embd, uint32_t n, uint32_t n_dim, const uint32_
                         if (gg > clip_val) gg = clip_val;
                         if (gg < -clip_val) gg = -clip_val;
                         g[d] += two * gg;
+                        ga[d] += fabs((double)(two * gg));
                     }
                 }
             }
@@ -581,10 +593,13 @@ void orc_grad_accum(const float *embd, uint32_t n, uint32_t n_dim, const uint32_
                 for (uint32_t d = 0; d < n_dim; d++) {
                     float delta = embd[base_self + d] - embd[base_k + d];
                     g[d] += grad_coeff * delta;
+                    ga[d] += fabs((double)(grad_coeff * delta));
                 }
             }
         }
         for (uint32_t d = 0; d < n_dim; d++) grad[base_self + d] = g[d];
+        if (abs_sum)
+            for (uint32_t d = 0; d < n_dim; d++) abs_sum[base_self + d] = ga[d];
         if (has_update) has_update[node] = active;
     }
 }

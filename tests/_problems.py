@@ -107,3 +107,51 @@ def config_oracle_graph(name, seed=2024):
     (r, c, v), sig, rho = O.construct_umap_graph(idx, dist, n_epochs)
     return dict(X=X, idx=idx, dist=dist, row=r, col=c, val=v, sigma=sig, rho=rho, ptr=O.coo_to_adj_ptr(n, r),
                 n=n, n_epochs=n_epochs)
+
+
+# Unit roundoff of f32 (2^-24): the scale of one rounding of an f32 sum,
+# relative to the magnitude of its terms.
+F32_U = 2.0 ** -24
+
+
+def adam_step64(g, m0, v0, fused, epsc, beta1, beta2):
+    """The Adam step of umap_adam_update (umap_optimiser_gpu.rs:912-922) in
+    f64 from the epoch's starting moments, and its derivative by g."""
+    g = np.asarray(g, np.float64)
+    m0 = np.asarray(m0, np.float64)
+    v0 = np.asarray(v0, np.float64)
+    m = m0 + (1.0 - beta1) * (g - m0)
+    v = v0 + (1.0 - beta2) * (g * g - v0)
+    sv = np.sqrt(v)
+    den = sv + np.float64(epsc)
+    step = np.float64(fused) * m / den
+    dv = 2.0 * (1.0 - beta2) * g
+    dsv = np.where(sv > 0, dv / (2.0 * np.maximum(sv, 1e-300)), 0.0)
+    dstep = np.float64(fused) * ((1.0 - beta1) / den - m * dsv / (den * den))
+    return step, dstep
+
+
+def update_errors(go, gg, abs_sum, m0, v0, fused, epsc, beta1, beta2, active, floor=0.1, units=64.0):
+    """Per-element comparison of the Adam steps two gradients imply (the
+    reference's go, the device's gg), over the active nodes' elements.
+    -> dict with
+      rel      : |s_dev - s_ref| / |s_ref| per element;
+      bound_ok : every element within 1e-5 |s_ref| + units * u * S * |ds/dg|,
+                 S = the sum of |terms| of the element's gradient (the scale
+                 of the reference's own f32 rounding of that sum, u = 2^-24):
+                 1e-5 relative, up to what cancellation in the gradient sum
+                 leaves undetermined;
+      floor_max: the largest rel among elements whose step is at least
+                 `floor` of the largest and whose gradient sum does not
+                 cancel (S <= 30 |g|)."""
+    act = np.asarray(active, bool)
+    s_ref, ds = adam_step64(go, m0, v0, fused, epsc, beta1, beta2)
+    s_dev, _ = adam_step64(gg, m0, v0, fused, epsc, beta1, beta2)
+    s_ref, ds, s_dev, S, g = s_ref[act], ds[act], s_dev[act], np.asarray(abs_sum)[act], np.asarray(go, np.float64)[act]
+    err = np.abs(s_dev - s_ref)
+    rel = err / np.maximum(np.abs(s_ref), 1e-300)
+    bound = 1e-5 * np.abs(s_ref) + units * F32_U * S * np.abs(ds)
+    sel = (np.abs(s_ref) >= floor * np.abs(s_ref).max()) & (S <= 30.0 * np.abs(g))
+    return dict(rel=rel.ravel(), bound_ok=bool((err <= bound).all()), worst_over_bound=float((err / bound).max()),
+                floor_max=float(rel[sel].max()) if sel.any() else 0.0, floor_count=int(sel.sum()),
+                count=int(rel.size))

@@ -97,21 +97,13 @@ def test_dens_state_parity_at_c3():
     assert st.mu_tot == pytest.approx(float(ref["mu_tot"]), rel=1e-6)
 
 
-def _adam_step64(g, m0, v0, fused, epsc, beta1, beta2):
-    """The Adam step of umap_adam_update (umap_optimiser_gpu.rs:912-922) in
-    f64, from the epoch's starting moments."""
-    g = g.astype(np.float64)
-    m = m0.astype(np.float64) + (1.0 - np.float64(beta1)) * (g - m0)
-    v = v0.astype(np.float64) + (1.0 - np.float64(beta2)) * (g * g - v0)
-    return np.float64(fused) * m / (np.sqrt(v) + np.float64(epsc))
-
-
-def epoch_update_errors(g, n_epochs, warm, checked, seed=42, floor=0.1):
+def epoch_update_errors(g, n_epochs, warm, checked, seed=42):
     """Epochs 0 .. warm + checked - 1 of a layout, the device and the oracle
     both starting every epoch from the oracle's state (embedding, moments,
-    cursors) with the same injected negatives; over the last `checked`
-    epochs -> (max relative error of the step on elements at least `floor`
-    of the epoch's largest step, quantiles over all active elements, count)."""
+    cursors) with the same injected negatives; the device's Adam is checked
+    bit for bit against the oracle's on the device's gradient, and the last
+    `checked` epochs' steps are compared (update_errors)."""
+    from tests._problems import update_errors
     n = g["n"]
     adj = umapcu.Adjacency(g["ptr"], g["col"], g["val"])
     p = umapcu.UmapOptimParams.from_min_dist_spread(0.1, 1.0, n_epochs=n_epochs, neg_sample_rate=5)
@@ -122,16 +114,17 @@ def epoch_update_errors(g, n_epochs, warm, checked, seed=42, floor=0.1):
     m = np.zeros_like(y)
     v = np.zeros_like(y)
     rng = np.random.default_rng(5)
-    worst, rels = 0.0, []
+    out = []
     for e in range(warm + checked):
         inj = rng.integers(0, n, (2 * csr["n_edges"], 5)).astype(np.uint32)
         y0, m0, v0 = y.copy(), m.copy(), v.copy()
         st.write(y0, m0, v0)
         gg, hu = st.epoch_debug(e, injected=inj)
         ye, me, ve, ce = st.read()
-        go, huo = O.grad_accum(y0, csr, cursor, e, seed, 5, p.a, p.b, p.gamma, injected=inj)
+        S = np.zeros((n, 2), np.float64)
+        go, huo = O.grad_accum(y0, csr, cursor, e, seed, 5, p.a, p.b, p.gamma, injected=inj, abs_sum=S)
         fused, epsc = O.adam_epoch_scalars(p.lr, p.beta1, p.beta2, p.eps, e, p.n_epochs)
-        # (a) the device's Adam is the reference's: the oracle's Adam fed the
+        # the device's Adam is the reference's: the oracle's Adam fed the
         # device's gradient lands on the device's state bit for bit
         ya, ma, va = y0.copy(), m0.copy(), v0.copy()
         O.adam_update(gg, huo, ma, va, ya, fused, epsc, p.beta1, p.beta2)
@@ -141,19 +134,11 @@ def epoch_update_errors(g, n_epochs, warm, checked, seed=42, floor=0.1):
         O.adam_update(go, huo, m, v, y, fused, epsc, p.beta1, p.beta2)
         O.schedule_update(csr["eps"], cursor, e)
         assert np.array_equal(ce, cursor)
-        if e < warm:
-            continue
-        # (b) the steps the two gradients imply, in f64
-        act = huo.astype(bool)
-        s_ref = _adam_step64(go, m0, v0, fused, epsc, p.beta1, p.beta2)[act]
-        s_dev = _adam_step64(gg, m0, v0, fused, epsc, p.beta1, p.beta2)[act]
-        rel = np.abs(s_dev - s_ref) / np.maximum(np.abs(s_ref), 1e-300)
-        big = np.abs(s_ref) >= floor * np.abs(s_ref).max()
-        worst = max(worst, float(rel[big].max()))
-        rels.append(rel)
+        if e >= warm:
+            act = np.repeat(huo.astype(bool)[:, None], 2, 1)
+            out.append(update_errors(go, gg, S, m0, v0, fused, epsc, p.beta1, p.beta2, act))
     st.close()
-    r = np.concatenate(rels)
-    return worst, np.quantile(r, [0.5, 0.99, 0.999]), r.size
+    return out
 
 
 @pytest.mark.parametrize("name,n_epochs,warm", [("c1", 500, 20), ("c2", 200, 6)])
@@ -163,19 +148,27 @@ def test_single_epoch_update_per_element(name, n_epochs, warm):
     both sides from the oracle's state; the reference's update is the
     oracle's mirror of umap_grad_accum (umap_optimiser_gpu.rs:682-860)
     through its Adam, the device's is the device's gradient through the
-    device's Adam.
-    (a) The device's Adam is the reference's bit for bit (asserted inside).
-    (b) The steps the two gradients imply, evaluated in f64 so that the f32
-    rounding of the embedding (an ulp of a coordinate near 10 is ~1e-6 of
-    the coordinate) does not hide them, agree within 1e-5 relative on every
-    element whose step is at least a tenth of the epoch's largest. Smaller
-    steps come from moments near zero -- the gradient changing sign -- where
-    the f32 sum of a node's attractive and repulsive terms carries a
-    relative error that no summation order bounds by 1e-5; their error
-    distribution is printed with the rest."""
+    device's Adam, which is the reference's Adam bit for bit (asserted). The
+    steps the two gradients imply are compared in f64, so that the f32
+    rounding of the embedding (an ulp of a coordinate near 10 is ~1e-6 of it)
+    does not hide them:
+    * on every element whose step is at least a tenth of the epoch's largest
+      and whose gradient sum does not cancel (sum of |terms| <= 30 |g|):
+      within 1e-5 relative;
+    * on every active element: within 1e-5 relative plus 64 units of the
+      reference's own f32 rounding of the element's gradient sum (2^-24 times
+      its sum of |terms|) carried into the step -- where the sum cancels, the
+      reference's f32 arithmetic itself does not determine the step to 1e-5.
+    The distribution is printed."""
     from tests._problems import config_oracle_graph
     g = config_oracle_graph(name)
-    worst, q, count = epoch_update_errors(g, n_epochs, warm, 2)
-    print(f"[epoch {name}] step rel err over {count} active elements: median {q[0]:.2e}, p99 {q[1]:.2e}, "
-          f"p99.9 {q[2]:.2e}; max where |step| >= 0.1 max: {worst:.2e}")
+    res = epoch_update_errors(g, n_epochs, warm, 2)
+    rel = np.concatenate([r["rel"] for r in res])
+    q = np.quantile(rel, [0.5, 0.99, 0.999])
+    worst = max(r["floor_max"] for r in res)
+    print(f"[epoch {name}] step rel err over {rel.size} active elements: median {q[0]:.2e}, p99 {q[1]:.2e}, "
+          f"p99.9 {q[2]:.2e}; max on the {sum(r['floor_count'] for r in res)} elements >= 0.1 max step without "
+          f"cancellation: {worst:.2e}; max err / (1e-5 rel + 64 roundings): "
+          f"{max(r['worst_over_bound'] for r in res):.3g}")
     assert worst <= 1e-5, worst
+    assert all(r["bound_ok"] for r in res)
