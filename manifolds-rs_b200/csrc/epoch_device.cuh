@@ -324,13 +324,14 @@ __device__ __forceinline__ unsigned process_batch(const EpochArgs &A, Smem &S, b
             if constexpr (DENS) {
                 // umap_optimiser_gpu.rs:769-798
                 const float4 dns = S.dn[j];
-                float phi = 1.0f / denom;
-                float dphi_term = A.a * A.b * dist_sq_b / dist_sq * phi;
+                const bool pr = !FAST && A.precise_pow;
+                float phi = div_k(1.0f, denom, pr);
+                float dphi_term = div_k(A.a * A.b * dist_sq_b, dist_sq, pr) * phi;
                 float common = 1.0f - A.b * (1.0f - phi);
-                float dr_self = (phi / dns.x) * (common / dns.y + dphi_term);
-                float dr_other = (phi / dno.x) * (common / dno.y + dphi_term);
+                float dr_self = div_k(phi, dns.x, pr) * (div_k(common, dns.y, pr) + dphi_term);
+                float dr_other = div_k(phi, dno.x, pr) * (div_k(common, dno.y, pr) + dphi_term);
                 float w_s = dens_weight(dns.z, dns.w, dstat), w_o = dens_weight(dno.z, dno.w, dstat);
-                float cor = dstat[4] * (w_s * dr_self + w_o * dr_other) / mu_e;
+                float cor = div_k(dstat[4] * (w_s * dr_self + w_o * dr_other), mu_e, pr);
                 float two_cor = 2.0f * cor;
 #pragma unroll
                 for (int d = 0; d < D; d++) c[d] += 2.0f * clip4(two_cor * (ys[d] - yo[d]));

@@ -44,7 +44,7 @@
 namespace umapcu {
 
 template <int D, bool DENS, int NR, bool FAST = false, bool LIST = false, bool BITS = false>
-__global__ void __launch_bounds__(kWarps * 32, (BITS && !DENS) ? 9 : 6) k_epoch(const EpochArgs A)
+__global__ void __launch_bounds__(kWarps * 32, 6) k_epoch(const EpochArgs A)
 {
     constexpr int KU = LIST ? 1 : kU;  // the list path keeps no scan queue
     __shared__ WarpSmem<D, KU, BITS> smem[kWarps];
@@ -82,8 +82,9 @@ __global__ void __launch_bounds__(kWarps * 32) k_epoch_split_bits(const EpochArg
 // ------------------------------------------------------------ densMAP
 
 constexpr int kDensBlock = 256;
-// Entries of a row taken together: their `other` loads, then their
-// coordinate gathers, are issued before any is used.
+// Entries of a segment are taken in super-chunks of kDensU x 32: all their
+// `other` loads, then all their coordinate gathers, are issued before any is
+// used.
 constexpr int kDensU = 4;
 
 struct DensSums {
@@ -96,11 +97,10 @@ struct DensSums {
 // then correlation_stats (density.rs:464-508) and the weight scalars of
 // launch_dens_update (umap_optimiser_gpu.rs:1123-1142) for the whole
 // embedding.
-// Radii: a thread per node, as the reference's kernel: the node walks its
-// row in CSR order and adds phi * d^2 and phi to its two f32 sums entry by
-// entry -- the reference's summation order -- with the other endpoints and
-// their coordinates for kDensU entries loaded before any is used (the row's
-// endpoint indices come through L1: neighbouring threads' rows are adjacent).
+// Radii: a warp per 32-node segment (the block's 8 warps cover its 256
+// nodes); lanes take consecutive CSR entries of the segment, and per-node
+// sums come from a segmented warp scan keyed by the entry's node, added to
+// the node's lane chunk by chunk.
 // Statistics: each block writes f64 sums of re, re^2, re * r and r over its
 // nodes (a fixed warp-tree order); the last block to finish (atomic ticket
 // after a fence) adds the blocks' sums in a fixed order and forms
@@ -113,52 +113,107 @@ template <int D>
 __global__ void __launch_bounds__(kDensBlock) k_dens_update(const DensArgs A)
 {
     constexpr int kW = kDensBlock / 32;
+    struct Seg {
+        uint32_t beg[33];
+        float ys[32][D];
+        float sums[32][2];
+    };
+    __shared__ Seg sm[kW];
     __shared__ DensSums shw[kW];
     __shared__ DensSums red[kDensBlock];
     __shared__ bool is_last;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t n = A.n;
-    const uint32_t node = blockIdx.x * kDensBlock + threadIdx.x;
+    Seg &S = sm[warp];
+    const uint32_t node0 = blockIdx.x * kDensBlock + warp * 32u;
+    const uint32_t node = node0 + lane;
     const bool valid = node < n;
-    uint32_t beg = 0, end = 0;
+    const uint32_t nc = min(node0, n);
+    S.beg[lane] = A.offsets[valid ? node : n];
+    if (lane == 31) S.beg[32] = A.offsets[min(nc + 32u, n)];
     float ys[D];
+    if (valid) load_row<D>(A.y, node, ys);
+    else {
 #pragma unroll
-    for (int d = 0; d < D; d++) ys[d] = 0.0f;
-    if (valid) {
-        beg = A.offsets[node];
-        end = A.offsets[node + 1];
-        if (!checked_ok(beg <= end && end <= A.n_entries, A.err)) end = beg;
-        load_row<D>(A.y, node, ys);
+        for (int d = 0; d < D; d++) ys[d] = 0.0f;
     }
+#pragma unroll
+    for (int d = 0; d < D; d++) S.ys[lane][d] = ys[d];
+    __syncwarp();
+#ifdef UMAPCU_CHECKED
+    {
+        const bool bad = S.beg[lane + 1] < S.beg[lane] || S.beg[lane + 1] > A.n_entries;
+        if (__any_sync(kFull, bad)) {
+            if (lane == 0) checked_ok(false, A.err);
+            __syncwarp();
+            S.beg[lane] = 0;
+            if (lane == 31) S.beg[32] = 0;
+        }
+        __syncwarp();
+    }
+#endif
+    const uint32_t seg_beg = S.beg[0], seg_end = S.beg[32];
     const uint64_t pol = l2_keep_policy();
     float sum_sq = 0.0f, sum_phi = 0.0f;
-    for (uint32_t p0 = beg; p0 < end; p0 += kDensU) {
+    for (uint32_t c0 = seg_beg; c0 < seg_end; c0 += 32u * kDensU) {
         uint32_t o[kDensU];
         float yo[kDensU][D];
-        bool in[kDensU];
 #pragma unroll
         for (int u = 0; u < kDensU; u++) {
-            in[u] = p0 + u < end;
-            o[u] = in[u] ? __ldg(A.other + p0 + u) : 0u;
+            const uint32_t p = c0 + 32u * u + lane;
+            o[u] = p < seg_end ? __ldcs(A.other + p) : 0u;
+        }
+        bool in_range[kDensU];
+#pragma unroll
+        for (int u = 0; u < kDensU; u++) {
+            const uint32_t p = c0 + 32u * u + lane;
+            in_range[u] = p < seg_end && checked_ok(o[u] < n, A.err);
+            if (in_range[u]) load_row_keep<D>(A.y, o[u], yo[u], pol);
         }
 #pragma unroll
         for (int u = 0; u < kDensU; u++) {
-            in[u] = in[u] && checked_ok(o[u] < n, A.err);
-            if (in[u]) load_row_keep<D>(A.y, o[u], yo[u], pol);
-        }
+            if (c0 + 32u * u >= seg_end) break;  // warp-uniform
+            const uint32_t p = c0 + 32u * u + lane;
+            const bool live = in_range[u];
+            uint32_t j = 32;
+            float t[2] = {0.0f, 0.0f};
+            if (live) {
+                j = local_node(S.beg, p);
+                float dist_sq = 0.0f;
 #pragma unroll
-        for (int u = 0; u < kDensU; u++) {
-            if (!in[u]) continue;
-            float dist_sq = 0.0f;
-#pragma unroll
-            for (int d = 0; d < D; d++) {
-                float diff = ys[d] - yo[u][d];
-                dist_sq += diff * diff;
+                for (int d = 0; d < D; d++) {
+                    float diff = S.ys[j][d] - yo[u][d];
+                    dist_sq += diff * diff;
+                }
+                float dist_sq_b = pow_pos(dist_sq, A.b, A.precise_pow);
+                float phi = div_k(1.0f, 1.0f + A.a * dist_sq_b, A.precise_pow);
+                t[0] = phi * dist_sq;
+                t[1] = phi;
             }
-            const float dist_sq_b = pow_pos(dist_sq, A.b, A.precise_pow);
-            const float phi = 1.0f / (1.0f + A.a * dist_sq_b);
-            sum_sq += phi * dist_sq;
-            sum_phi += phi;
+            const uint32_t jprev = __shfl_up_sync(kFull, j, 1);
+            const uint32_t jnext = __shfl_down_sync(kFull, j, 1);
+            const unsigned heads = __ballot_sync(kFull, lane == 0 || jprev != j);
+            const int start = 31 - __clz(heads & (lane == 31 ? kFull : ((2u << lane) - 1u)));
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+#pragma unroll
+                for (int q = 0; q < 2; q++) {
+                    const float v = __shfl_up_sync(kFull, t[q], off);
+                    if (lane - off >= start) t[q] += v;
+                }
+            }
+            const bool tail = live && (lane == 31 || jnext != j);
+            if (tail) {
+                S.sums[j][0] = t[0];
+                S.sums[j][1] = t[1];
+            }
+            const unsigned has = __reduce_or_sync(kFull, tail ? (1u << j) : 0u);
+            __syncwarp();
+            if ((has >> lane) & 1u) {
+                sum_sq += S.sums[lane][0];
+                sum_phi += S.sums[lane][1];
+            }
+            __syncwarp();
         }
     }
     DensSums v{0.0, 0.0, 0.0, 0.0};

@@ -456,7 +456,9 @@ void umapcu_server::tick_launch()
         P.scal = G.scal.p + j->sc_off;
         P.bits = G.bits.p;
         P.bits_words = G.bits_words;
-        P.n_entries = 2 * j->n_edges;
+        // the length of the group's entry arrays: the job's offsets index
+        // them group-wide
+        P.n_entries = 2 * G.csr.n_edges;
         const umapcu_optim_params &q = j->params;
         P.a = q.a;
         P.b = q.b;

@@ -258,7 +258,6 @@ def test_single_epoch_injected_negatives(n_dim, precise, nr):
         act = np.repeat(huo.astype(bool)[:, None], n_dim, 1)
         r = update_errors(go, gg, S, m0, v0, fused, epsc, p.beta1, p.beta2, act)
         assert r["floor_max"] <= 1e-5 and r["bound_ok"], (e, r["floor_max"], r["worst_over_bound"])
-        assert np.abs(ye - y).max() <= 1e-5 * np.abs(y).max()
 
 
 def test_single_epoch_update_from_reference_state():
