@@ -229,6 +229,7 @@ umapcu_status create_state(const float *embd, uint32_t n, uint32_t n_dim, const 
     st->seed = seed;
     st->sampler = sampler;
     {
+        NvtxRange r("umapcu graph upload + CSR build");
         DevBuf<uint64_t> dptr(n + 1, s);
         DevBuf<uint32_t> dcol(nnz, s);
         DevBuf<float> dw(nnz, s);
@@ -246,6 +247,7 @@ umapcu_status create_state(const float *embd, uint32_t n, uint32_t n_dim, const 
     // lists do not fit) takes the bitmasks, built in well under a millisecond.
     // UMAPCU_NO_SCHEDULE_LISTS set: neither, every epoch scans the cursors.
     const bool precompute = !getenv("UMAPCU_NO_SCHEDULE_LISTS");
+    NvtxRange r_sched("umapcu schedule precompute");
     if (lists && precompute) {
         sync(s);
         const auto t0 = std::chrono::steady_clock::now();
@@ -461,6 +463,7 @@ umapcu_status umapcu_construct_umap_graph(const int32_t *knn_idx, const float *k
         if (!row || !col || !val) return UMAPCU_BAD_ARG;
         for (uint64_t i = 0; i < nk; i++)
             if (knn_idx[i] < 0 || (uint32_t)knn_idx[i] >= n) return UMAPCU_BAD_ARG;
+        NvtxRange r("umapcu construct_umap_graph");
         Stream S;
         DevBuf<int32_t> di(nk, S.s);
         DevBuf<float> dd(nk, S.s), sg(n, S.s), rh(n, S.s);
@@ -566,6 +569,7 @@ umapcu_status umapcu_state_run(umapcu_state *st, uint32_t first_epoch, uint32_t 
 {
     return guard([&]() -> umapcu_status {
         if (!st || optimiser > UMAPCU_OPT_SGD) return UMAPCU_BAD_ARG;
+        NvtxRange r("umapcu state run");
         for (uint32_t e = first_epoch; e < first_epoch + count; e++) run_epoch(st, e, optimiser, nullptr, nullptr, nullptr);
         sync(st->stream.s);
         return take_error(st);
@@ -764,6 +768,7 @@ umapcu_status umapcu_optimise_embedding(float *embd, uint32_t n, uint32_t n_dim,
                    optimiser == UMAPCU_OPT_SGD ? "SGD" : "Adam");
         const uint64_t nt = (uint64_t)n * n_dim;
         PhaseTimer T;
+        NvtxRange r("umapcu epochs");
         for (uint32_t e = 0; e < params->n_epochs; e++) {
             const bool log_now = verbose && ((e + 1) % 100 == 0 || e + 1 == params->n_epochs);
             if (!log_now) {

@@ -369,6 +369,7 @@ umapcu_status umapcu_batch_run(umapcu_batch *b, uint32_t mode, float *ms)
 {
     return guard_b([&]() -> umapcu_status {
         if (!b || mode > 2) return UMAPCU_BAD_ARG;
+        NvtxRange r("umapcu batch run");
         BatchConfig c = b->cfg;
         if (mode == 0 && !b->tuned) autotune(b);
         if (mode == 0) c = b->cfg;

@@ -11,9 +11,21 @@
 #include <stdexcept>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "umapcu.h"
 
 namespace umapcu {
+
+// A named NVTX range for the scope (stages of the entry points: graph, CSR
+// build, schedule, epochs, admission, ticks, ...). Header-only NVTX: without
+// a profiler attached a range costs a function call and nothing else.
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
 
 // Internal error carrier: thrown inside the library, caught at the C ABI.
 struct Error {

@@ -291,6 +291,7 @@ void umapcu_server::answer_snapshots(const std::vector<ServeJob *> &done)
 // in shared buffers (stream of admission thread k).
 void umapcu_server::admit_group(std::vector<ServeJob *> &g, int k)
 {
+    NvtxRange r("umapcu admit group");
     cudaStream_t s = own2[k].s;
     const uint32_t J = (uint32_t)g.size();
     uint64_t n_tot = 0, nnz = 0, y_tot = 0, sc_tot = 0;
@@ -433,6 +434,7 @@ void umapcu_server::group_job_done(ServeJob *j)
 // Enqueues one tick over the active jobs on stream s (asynchronous).
 void umapcu_server::tick_launch()
 {
+    NvtxRange r("umapcu tick");
     hp.assign(active.size(), BatchProblem{});
     segs.clear();
     bool nr5 = true, all_hash = true;
