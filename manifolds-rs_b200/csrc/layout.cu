@@ -81,15 +81,62 @@ __global__ void __launch_bounds__(kWarps * 32) k_epoch_split_bits(const EpochArg
 
 // ------------------------------------------------------------ densMAP
 
-constexpr int kDensBlock = 256;
-// Entries of a segment are taken in super-chunks of kDensU x 32: all their
-// `other` loads, then all their coordinate gathers, are issued before any is
-// used.
-constexpr int kDensU = 4;
+constexpr int kDensBlock = 128;
+// Consecutive CSR entries a lane takes per window: 8 for 1-2 dimensions, 4
+// above (the coordinate gathers of a piece are held in registers together).
+template <int D>
+struct DensPiece {
+    static constexpr int P = D <= 2 ? 8 : 4;
+};
 
 struct DensSums {
     double s_re, s_re2, s_rer, s_r;
 };
+
+__device__ __forceinline__ void dens_sums_add(DensSums &a, const DensSums &b)
+{
+    a.s_re += b.s_re;
+    a.s_re2 += b.s_re2;
+    a.s_rer += b.s_rer;
+    a.s_r += b.s_r;
+}
+
+__device__ __forceinline__ DensSums dens_sums_warp(DensSums v)
+{
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        v.s_re += __shfl_down_sync(kFull, v.s_re, off);
+        v.s_re2 += __shfl_down_sync(kFull, v.s_re2, off);
+        v.s_rer += __shfl_down_sync(kFull, v.s_rer, off);
+        v.s_r += __shfl_down_sync(kFull, v.s_r, off);
+    }
+    return v;
+}
+
+// The `other` endpoints of CSR entries [a, a + P) into o[]: two (P = 8) or
+// one (P = 4) 16-byte loads where the array is 16-byte aligned and the
+// piece lies inside it, else entry by entry inside [lo, hi).
+template <int P>
+__device__ __forceinline__ void dens_load_piece(const uint32_t *__restrict__ other, uint64_t n_entries, bool vec,
+                                                uint32_t a, uint32_t lo, uint32_t hi, uint32_t (&o)[P])
+{
+    if (vec && (uint64_t)a + P <= n_entries) {
+#pragma unroll
+        for (int h = 0; h < P / 4; h++) {
+            const uint4 q = __ldcs(reinterpret_cast<const uint4 *>(other + a) + h);
+            o[4 * h] = q.x;
+            o[4 * h + 1] = q.y;
+            o[4 * h + 2] = q.z;
+            o[4 * h + 3] = q.w;
+        }
+    } else {
+#pragma unroll
+        for (int u = 0; u < P; u++) {
+            const uint32_t p = a + u;
+            o[u] = (p >= lo && p < hi) ? __ldcs(other + p) : 0u;
+        }
+    }
+}
 
 // One densMAP update in one launch: umap_dens_radii (umap_optimiser_gpu.rs:
 // 503-543) per node -- over all its CSR entries, phi = 1 / (1 + a d^2b),
@@ -97,10 +144,20 @@ struct DensSums {
 // then correlation_stats (density.rs:464-508) and the weight scalars of
 // launch_dens_update (umap_optimiser_gpu.rs:1123-1142) for the whole
 // embedding.
-// Radii: a warp per 32-node segment (the block's 8 warps cover its 256
-// nodes); lanes take consecutive CSR entries of the segment, and per-node
-// sums come from a segmented warp scan keyed by the entry's node, added to
-// the node's lane chunk by chunk.
+// Radii: a warp per 32-node segment, walked in windows of 32 P consecutive
+// CSR entries (P = DensPiece<D>::P, windows aligned to P): lane l takes the
+// window's piece [w0 + l P, w0 + (l + 1) P). A lane loads its piece's
+// endpoints with 16-byte loads (the next window's while the current one
+// computes), gathers their coordinates together, then walks the piece in
+// CSR order, its node found once by a search of the row starts and
+// advanced at each row start it passes. A piece yields a partial (sum of
+// phi * d^2, sum of phi) per node it touches: the first node's (h) and the
+// last node's (t) stay in the lane's registers, those of nodes wholly
+// inside the piece go to the node's shared slot C. The h of consecutive
+// pieces that start in the same node are summed by a segmented warp scan,
+// and node lane j adds its row's part of the window -- t of its first
+// piece plus the run sum, or one partial -- to its sums. Every addition
+// has a fixed order.
 // Statistics: each block writes f64 sums of re, re^2, re * r and r over its
 // nodes (a fixed warp-tree order); the last block to finish (atomic ticket
 // after a fence) adds the blocks' sums in a fixed order and forms
@@ -109,18 +166,19 @@ struct DensSums {
 // moments in one pass, equal to them to f64 rounding -- then writes
 // stats = {mean, std, cov, 1 / std^2, lambda * mu_tot / (std * (n - 1))} in
 // f32 and re-arms the ticket for the next launch.
-template <int D>
+template <int D, bool PRECISE>
 __global__ void __launch_bounds__(kDensBlock) k_dens_update(const DensArgs A)
 {
     constexpr int kW = kDensBlock / 32;
+    constexpr int P = DensPiece<D>::P;
+    constexpr uint32_t kWin = 32u * P;
     struct Seg {
         uint32_t beg[33];
         float ys[32][D];
-        float sums[32][2];
+        float2 C[32];  // partials of nodes wholly inside one piece
     };
     __shared__ Seg sm[kW];
     __shared__ DensSums shw[kW];
-    __shared__ DensSums red[kDensBlock];
     __shared__ bool is_last;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t n = A.n;
@@ -131,14 +189,12 @@ __global__ void __launch_bounds__(kDensBlock) k_dens_update(const DensArgs A)
     const uint32_t nc = min(node0, n);
     S.beg[lane] = A.offsets[valid ? node : n];
     if (lane == 31) S.beg[32] = A.offsets[min(nc + 32u, n)];
-    float ys[D];
-    if (valid) load_row<D>(A.y, node, ys);
-    else {
+    if (valid) {
+        float ys[D];
+        load_row<D>(A.y, node, ys);
 #pragma unroll
-        for (int d = 0; d < D; d++) ys[d] = 0.0f;
+        for (int d = 0; d < D; d++) S.ys[lane][d] = ys[d];
     }
-#pragma unroll
-    for (int d = 0; d < D; d++) S.ys[lane][d] = ys[d];
     __syncwarp();
 #ifdef UMAPCU_CHECKED
     {
@@ -153,68 +209,124 @@ __global__ void __launch_bounds__(kDensBlock) k_dens_update(const DensArgs A)
     }
 #endif
     const uint32_t seg_beg = S.beg[0], seg_end = S.beg[32];
+    const uint32_t my_beg = S.beg[lane], my_end = S.beg[lane + 1];
+    const bool vec = (reinterpret_cast<uintptr_t>(A.other) & 15u) == 0;
     const uint64_t pol = l2_keep_policy();
-    float sum_sq = 0.0f, sum_phi = 0.0f;
-    for (uint32_t c0 = seg_beg; c0 < seg_end; c0 += 32u * kDensU) {
-        uint32_t o[kDensU];
-        float yo[kDensU][D];
+    float sum_sq = 0.0f, sum_phi = 0.0f;  // node lane's sums
+    uint32_t w0 = seg_beg & ~(uint32_t)(P - 1);
+    uint32_t o[P];
+    if (w0 < seg_end) dens_load_piece<P>(A.other, A.n_entries, vec, w0 + lane * P, seg_beg, seg_end, o);
+    for (; w0 < seg_end; w0 += kWin) {
+        const uint32_t a = w0 + (uint32_t)lane * P;
+        // this piece's coordinate gathers, all in flight together
+        float yo[P][D];
+        bool in[P];
 #pragma unroll
-        for (int u = 0; u < kDensU; u++) {
-            const uint32_t p = c0 + 32u * u + lane;
-            o[u] = p < seg_end ? __ldcs(A.other + p) : 0u;
+        for (int u = 0; u < P; u++) {
+            const uint32_t p = a + u;
+            in[u] = p >= seg_beg && p < seg_end;
+            in[u] = in[u] && checked_ok(o[u] < n, A.err);
+            if (in[u]) load_row_keep<D>(A.y, o[u], yo[u], pol);
         }
-        bool in_range[kDensU];
+        // the next window's endpoints, in flight while this one computes
+        if (w0 + kWin < seg_end)
+            dens_load_piece<P>(A.other, A.n_entries, vec, a + kWin, seg_beg, seg_end, o);
+        // the piece in CSR order
+        uint32_t j = local_node(S.beg, a);
+        const uint32_t j_first = j;
+        uint32_t nxt = S.beg[j + 1];
+        float yj[D];
 #pragma unroll
-        for (int u = 0; u < kDensU; u++) {
-            const uint32_t p = c0 + 32u * u + lane;
-            in_range[u] = p < seg_end && checked_ok(o[u] < n, A.err);
-            if (in_range[u]) load_row_keep<D>(A.y, o[u], yo[u], pol);
-        }
+        for (int d = 0; d < D; d++) yj[d] = S.ys[j][d];
+        float ps = 0.0f, pp = 0.0f;
+        float2 hf = make_float2(0.0f, 0.0f);  // the first node's partial, once closed
+        bool first = true;
 #pragma unroll
-        for (int u = 0; u < kDensU; u++) {
-            if (c0 + 32u * u >= seg_end) break;  // warp-uniform
-            const uint32_t p = c0 + 32u * u + lane;
-            const bool live = in_range[u];
-            uint32_t j = 32;
-            float t[2] = {0.0f, 0.0f};
-            if (live) {
-                j = local_node(S.beg, p);
+        for (int u = 0; u < P; u++) {
+            const uint32_t p = a + u;
+            if (in[u] && p >= nxt) {  // a later node's row starts here
+                if (first) hf = make_float2(ps, pp);
+                else S.C[j] = make_float2(ps, pp);
+                first = false;
+                ps = pp = 0.0f;
+                do j++;
+                while (p >= S.beg[j + 1]);
+                nxt = S.beg[j + 1];
+#pragma unroll
+                for (int d = 0; d < D; d++) yj[d] = S.ys[j][d];
+            }
+            if (in[u]) {
                 float dist_sq = 0.0f;
 #pragma unroll
                 for (int d = 0; d < D; d++) {
-                    float diff = S.ys[j][d] - yo[u][d];
+                    const float diff = yj[d] - yo[u][d];
                     dist_sq += diff * diff;
                 }
-                float dist_sq_b = pow_pos(dist_sq, A.b, A.precise_pow);
-                float phi = div_k(1.0f, 1.0f + A.a * dist_sq_b, A.precise_pow);
-                t[0] = phi * dist_sq;
-                t[1] = phi;
+                const float dist_sq_b = pow_pos(dist_sq, A.b, PRECISE);
+                const float phi = div_k(1.0f, 1.0f + A.a * dist_sq_b, PRECISE);
+                ps += phi * dist_sq;
+                pp += phi;
             }
-            const uint32_t jprev = __shfl_up_sync(kFull, j, 1);
-            const uint32_t jnext = __shfl_down_sync(kFull, j, 1);
-            const unsigned heads = __ballot_sync(kFull, lane == 0 || jprev != j);
-            const int start = 31 - __clz(heads & (lane == 31 ? kFull : ((2u << lane) - 1u)));
-#pragma unroll
-            for (int off = 1; off < 32; off <<= 1) {
-#pragma unroll
-                for (int q = 0; q < 2; q++) {
-                    const float v = __shfl_up_sync(kFull, t[q], off);
-                    if (lane - off >= start) t[q] += v;
-                }
-            }
-            const bool tail = live && (lane == 31 || jnext != j);
-            if (tail) {
-                S.sums[j][0] = t[0];
-                S.sums[j][1] = t[1];
-            }
-            const unsigned has = __reduce_or_sync(kFull, tail ? (1u << j) : 0u);
-            __syncwarp();
-            if ((has >> lane) & 1u) {
-                sum_sq += S.sums[lane][0];
-                sum_phi += S.sums[lane][1];
-            }
-            __syncwarp();
         }
+        // this piece's first node's partial (h), and its last node's (t) when
+        // that is another node
+        float hx = ps, hy = pp, tx = 0.0f, ty = 0.0f;
+        if (!first) {
+            hx = hf.x;
+            hy = hf.y;
+            tx = ps;
+            ty = pp;
+        }
+        // h summed over each run of pieces that start in the same node
+        // (a segmented inclusive scan over the lanes; the first nodes do not
+        // decrease with the lane, so equal keys at lane - off mean one run)
+        float sx = hx, sy = hy;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const float ux = __shfl_up_sync(kFull, sx, off), uy = __shfl_up_sync(kFull, sy, off);
+            const uint32_t uk = __shfl_up_sync(kFull, j_first, off);
+            if (lane >= off && uk == j_first) {
+                sx = ux + sx;
+                sy = uy + sy;
+            }
+        }
+        __syncwarp();  // the C slots written above
+        // node lane: its row's part of this window. Pieces l0 .. l1 hold it:
+        // one piece -- that piece's h, t or the node's C slot; several -- the
+        // last node's t of piece l0 (unless the node starts piece l0) and the
+        // run sum at piece l1
+        const uint32_t lo = max(my_beg, w0), hi = min(my_end, w0 + kWin);
+        const bool mine = lo < hi;
+        const uint32_t l0 = mine ? (lo - w0) / P : (uint32_t)lane, l1 = mine ? (hi - 1 - w0) / P : (uint32_t)lane;
+        const uint32_t f0 = __shfl_sync(kFull, j_first, l0), e0 = __shfl_sync(kFull, j, l0);
+        const float h0x = __shfl_sync(kFull, hx, l0), h0y = __shfl_sync(kFull, hy, l0);
+        const float t0x = __shfl_sync(kFull, tx, l0), t0y = __shfl_sync(kFull, ty, l0);
+        const float s1x = __shfl_sync(kFull, sx, l1), s1y = __shfl_sync(kFull, sy, l1);
+        if (mine) {
+            float vx, vy;
+            if (l0 == l1) {
+                if (f0 == (uint32_t)lane) {
+                    vx = h0x;
+                    vy = h0y;
+                } else if (e0 == (uint32_t)lane) {
+                    vx = t0x;
+                    vy = t0y;
+                } else {
+                    const float2 c = S.C[lane];
+                    vx = c.x;
+                    vy = c.y;
+                }
+            } else if (f0 == (uint32_t)lane) {
+                vx = s1x;
+                vy = s1y;
+            } else {
+                vx = t0x + s1x;
+                vy = t0y + s1y;
+            }
+            sum_sq += vx;
+            sum_phi += vy;
+        }
+        __syncwarp();
     }
     DensSums v{0.0, 0.0, 0.0, 0.0};
     if (valid) {
@@ -227,23 +339,12 @@ __global__ void __launch_bounds__(kDensBlock) k_dens_update(const DensArgs A)
         v = DensSums{red_, red_ * red_, red_ * rd, rd};
     }
     // block sums, fixed order: warp tree, then the block's warps in order
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-        v.s_re += __shfl_down_sync(kFull, v.s_re, off);
-        v.s_re2 += __shfl_down_sync(kFull, v.s_re2, off);
-        v.s_rer += __shfl_down_sync(kFull, v.s_rer, off);
-        v.s_r += __shfl_down_sync(kFull, v.s_r, off);
-    }
+    v = dens_sums_warp(v);
     if (lane == 0) shw[warp] = v;
     __syncthreads();
     if (threadIdx.x == 0) {
         DensSums acc{0.0, 0.0, 0.0, 0.0};
-        for (int w = 0; w < kW; w++) {
-            acc.s_re += shw[w].s_re;
-            acc.s_re2 += shw[w].s_re2;
-            acc.s_rer += shw[w].s_rer;
-            acc.s_r += shw[w].s_r;
-        }
+        for (int w = 0; w < kW; w++) dens_sums_add(acc, shw[w]);
         double *pp = A.part + 4ull * blockIdx.x;
         pp[0] = acc.s_re;
         pp[1] = acc.s_re2;
@@ -255,8 +356,8 @@ __global__ void __launch_bounds__(kDensBlock) k_dens_update(const DensArgs A)
     __syncthreads();
     if (!is_last) return;
     __threadfence();
-    // the last block: every block's sums, a fixed order per thread, then a
-    // fixed tree over the threads
+    // the last block: every block's sums, a fixed order per thread, then the
+    // warp tree and the warps in order
     DensSums acc{0.0, 0.0, 0.0, 0.0};
     for (uint32_t b = threadIdx.x; b < gridDim.x; b += kDensBlock) {
         const double *pp = A.part + 4ull * b;
@@ -265,19 +366,12 @@ __global__ void __launch_bounds__(kDensBlock) k_dens_update(const DensArgs A)
         acc.s_rer += __ldcg(pp + 2);
         acc.s_r += __ldcg(pp + 3);
     }
-    red[threadIdx.x] = acc;
+    acc = dens_sums_warp(acc);
+    if (lane == 0) shw[warp] = acc;
     __syncthreads();
-    for (int w = kDensBlock / 2; w > 0; w >>= 1) {
-        if ((int)threadIdx.x < w) {
-            red[threadIdx.x].s_re += red[threadIdx.x + w].s_re;
-            red[threadIdx.x].s_re2 += red[threadIdx.x + w].s_re2;
-            red[threadIdx.x].s_rer += red[threadIdx.x + w].s_rer;
-            red[threadIdx.x].s_r += red[threadIdx.x + w].s_r;
-        }
-        __syncthreads();
-    }
     if (threadIdx.x == 0) {
-        const DensSums t = red[0];
+        DensSums t{0.0, 0.0, 0.0, 0.0};
+        for (int w = 0; w < kW; w++) dens_sums_add(t, shw[w]);
         const double nn = (double)(n > 1 ? n : 1);
         const double denom = (double)(n > 2 ? n - 1 : 1);
         const double mean = t.s_re / nn;
@@ -350,9 +444,10 @@ void launch_epoch(const EpochArgs &A, uint32_t n_dim, bool dens, cudaStream_t s)
 void launch_dens_update(const DensArgs &Dn, uint32_t n_dim, cudaStream_t s)
 {
     const uint32_t nb = ceil_div(Dn.n, kDensBlock);
-#define UMAPCU_CASE(DD)                                           \
-    case DD:                                                      \
-        k_dens_update<DD><<<nb, kDensBlock, 0, s>>>(Dn);          \
+#define UMAPCU_CASE(DD)                                                   \
+    case DD:                                                              \
+        if (Dn.precise_pow) k_dens_update<DD, true><<<nb, kDensBlock, 0, s>>>(Dn); \
+        else k_dens_update<DD, false><<<nb, kDensBlock, 0, s>>>(Dn);       \
         break;
     switch (n_dim) {
         UMAPCU_CASE(1) UMAPCU_CASE(2) UMAPCU_CASE(3) UMAPCU_CASE(4)
