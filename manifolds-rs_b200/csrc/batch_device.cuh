@@ -85,7 +85,7 @@ __device__ __forceinline__ void epoch_args_of(const BatchProblem &P, uint32_t e,
 template <int D, int NR, int KU, bool FAST = false, bool BITS = false>
 __global__ void __launch_bounds__(kWarps * 32, 8) k_batch_persistent(const BatchArgs B)
 {
-    __shared__ WarpSmem<D, KU, BITS> smem[kWarps];
+    __shared__ WarpSmem<D, KU, BITS, false> smem[kWarps];
     __shared__ EpochArgs sargs[kWarps];  // per-warp arguments of the current item (kept out of registers)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t total = B.n_epochs * B.n_segs;
@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(kWarps * 32, 8) k_batch_persistent(const Batch
 template <int D, int NR, int KU, bool FAST = false, bool BITS = false>
 __global__ void __launch_bounds__(kWarps * 32, 8) k_batch_epoch(const BatchArgs B, uint32_t e)
 {
-    __shared__ WarpSmem<D, KU, BITS> smem[kWarps];
+    __shared__ WarpSmem<D, KU, BITS, false> smem[kWarps];
     __shared__ EpochArgs sargs[kWarps];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t s = blockIdx.x * kWarps + warp;

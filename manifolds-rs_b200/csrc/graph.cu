@@ -312,19 +312,43 @@ __device__ __forceinline__ uint32_t row_of(const uint64_t *__restrict__ ptr, uin
     return lo;
 }
 
-// Upper-triangle entries (i < j) become edges. A column outside [0, n) is
-// reported in *bad and its entry dropped (the reference indexes out of range).
-__global__ void k_upper_flags(const uint64_t *__restrict__ adj_ptr, const uint32_t *__restrict__ adj_col,
-                              uint32_t n, uint64_t nnz, uint32_t *__restrict__ src_row, uint32_t *__restrict__ flag,
-                              uint32_t *__restrict__ bad)
+// Upper-triangle entries (i < j) become edges. A warp per segment of 32
+// rows: lane l holds the first entry of row r0 + l, and each entry of the
+// segment finds its row among them by a search over the lanes (the last row
+// starting at or before it, as row_of; entries before ptr[0] belong to row
+// 0). A column outside [0, n) is reported in *bad and its entry dropped (the
+// reference indexes out of range); so are row starts out of order, with
+// which the segments would not cover the entries once each.
+__global__ void __launch_bounds__(256) k_upper_flags(const uint64_t *__restrict__ adj_ptr,
+                                                     const uint32_t *__restrict__ adj_col, uint32_t n, uint64_t nnz,
+                                                     uint32_t *__restrict__ src_row, uint32_t *__restrict__ flag,
+                                                     uint32_t *__restrict__ bad)
 {
-    uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= nnz) return;
-    uint32_t i = row_of(adj_ptr, n, p);
-    const uint32_t c = adj_col[p];
-    src_row[p] = i;
-    if (c >= n) *bad = 1u;
-    flag[p] = i < c && c < n;
+    const unsigned full = 0xFFFFFFFFu;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t r0 = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32u;
+    if (r0 >= n) return;  // warp-uniform
+    const uint32_t rows = min(32u, n - r0);
+    const uint64_t start = adj_ptr[r0 + min(lane, rows)], seg_end = adj_ptr[r0 + rows];
+    const uint64_t next = __shfl_down_sync(full, start, 1);
+    const uint64_t row_end = lane + 1 < rows ? next : seg_end;
+    if (lane < rows && row_end < start) *bad = 1u;
+    const uint64_t b = r0 == 0 ? 0 : __shfl_sync(full, start, 0), e = min(seg_end, nnz);
+    for (uint64_t p0 = b; p0 < e; p0 += 32) {  // warp-uniform
+        const uint64_t p = p0 + lane;
+        uint32_t lo = 0;
+#pragma unroll
+        for (uint32_t step = 16; step > 0; step >>= 1) {
+            const uint64_t s = __shfl_sync(full, start, lo + step);
+            if (lo + step < rows && s <= p) lo += step;
+        }
+        if (p < e) {
+            const uint32_t i = r0 + lo, c = adj_col[p];
+            src_row[p] = i;
+            if (c >= n) *bad = 1u;
+            flag[p] = i < c && c < n;
+        }
+    }
 }
 
 __global__ void k_edges(const uint32_t *__restrict__ src_row, const uint32_t *__restrict__ adj_col,
@@ -413,7 +437,7 @@ umapcu_status build_csr_dev(uint32_t n, const uint64_t *d_adj_ptr, const uint32_
     DevBuf<uint32_t> src_row(nnz, s), flag(nnz, s), pos(nnz, s), bad(1, s);
     check_cuda(cudaMemsetAsync(bad.p, 0, sizeof(uint32_t), s), "memset");
     if (nnz) {
-        k_upper_flags<<<ceil_div(nnz, 256), 256, 0, s>>>(d_adj_ptr, d_adj_col, n, nnz, src_row.p, flag.p, bad.p);
+        k_upper_flags<<<ceil_div(n, 256), 256, 0, s>>>(d_adj_ptr, d_adj_col, n, nnz, src_row.p, flag.p, bad.p);
         check_launch("k_upper_flags");
     }
     uint32_t bad_h = 0;

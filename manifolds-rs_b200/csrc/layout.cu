@@ -47,7 +47,7 @@ template <int D, bool DENS, int NR, bool FAST = false, bool LIST = false, bool B
 __global__ void __launch_bounds__(kWarps * 32, 6) k_epoch(const EpochArgs A)
 {
     constexpr int KU = LIST ? 1 : kU;  // the list path keeps no scan queue
-    __shared__ WarpSmem<D, KU, BITS> smem[kWarps];
+    __shared__ WarpSmem<D, KU, BITS, DENS> smem[kWarps];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t node0 = (blockIdx.x * kWarps + warp) * 32u;
     if (node0 >= A.n) return;
@@ -59,7 +59,7 @@ __global__ void __launch_bounds__(kWarps * 32, 6) k_epoch(const EpochArgs A)
 template <int D, bool DENS, int NR, bool FAST>
 __global__ void __launch_bounds__(kWarps * 32) k_epoch_split(const EpochArgs A)
 {
-    __shared__ WarpSmem<D, 1> seg;
+    __shared__ WarpSmem<D, 1, false, DENS> seg;
     __shared__ float part[kWarps][32][D];
     __shared__ unsigned has_w[kWarps];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -71,7 +71,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_epoch_split(const EpochArgs A)
 template <int D, bool DENS, int NR, bool FAST>
 __global__ void __launch_bounds__(kWarps * 32) k_epoch_split_bits(const EpochArgs A)
 {
-    __shared__ WarpSmem<D, kU, true> seg;
+    __shared__ WarpSmem<D, kU, true, DENS> seg;
     __shared__ float part[kWarps][32][D];
     __shared__ unsigned has_w[kWarps];
     __shared__ uint32_t wm[kSplitWords], pre[kSplitWords + 1];
