@@ -150,6 +150,8 @@ void run_epoch(umapcu_state *st, uint32_t epoch, uint32_t optimiser, const uint3
     } else if (use_bits) {
         A.bits = st->bits.bits + (size_t)epoch * st->bits.words;
         st->sched_lazy = true;
+        if (st->bits.rest && epoch >= st->bits.first)  // the later epochs' words (build_schedule_bits)
+            check_cuda(cudaStreamWaitEvent(st->stream.s, st->bits.rest, 0), "cudaStreamWaitEvent");
     }
     if (in_order) st->sched_epoch = epoch + 1;
     A.n = st->n;
@@ -229,17 +231,27 @@ umapcu_status create_state(const float *embd, uint32_t n, uint32_t n_dim, const 
     st->seed = seed;
     st->sampler = sampler;
     {
+        // The row pointers and columns go first; the weights follow on a
+        // second stream while the CSR's structure is built from the former
+        // (build_csr_structure), and the weights phase waits for them.
         NvtxRange r("umapcu graph upload + CSR build");
         DevBuf<uint64_t> dptr(n + 1, s);
         DevBuf<uint32_t> dcol(nnz, s);
         DevBuf<float> dw(nnz, s);
+        Event col_in, w_in;
+        Stream side;  // declared after dw: on unwinding it is synchronised before dw is freed
         h2d(dptr.p, adj_ptr, n + 1, s);
         h2d(dcol.p, adj_col, nnz, s);
-        h2d(dw.p, adj_w, nnz, s);
-        T.mark("graph H2D", s);
-        umapcu_status rc = build_csr_dev(n, dptr.p, dcol.p, dw.p, nnz, st->csr, s);
+        col_in.record(s);
+        check_cuda(cudaStreamWaitEvent(side.s, col_in.e, 0), "cudaStreamWaitEvent");
+        h2d(dw.p, adj_w, nnz, side.s);
+        w_in.record(side.s);
+        CsrBuild tmp;
+        const umapcu_status rc = build_csr_structure(n, dptr.p, dcol.p, nnz, st->csr, tmp, s);
+        check_cuda(cudaStreamWaitEvent(s, w_in.e, 0), "cudaStreamWaitEvent");  // dw is freed on s
         if (rc != UMAPCU_OK) return rc;
-        T.mark("CSR build", s);
+        build_csr_weights(dw.p, st->csr, tmp, s);
+        T.mark("graph H2D + CSR build", s);
     }
     // The schedule precomputed for epochs 0 .. n_epochs - 1 (schedule.cu):
     // record lists pay for their build (~10 ms at 1M points) over repeated or

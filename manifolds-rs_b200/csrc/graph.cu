@@ -428,8 +428,94 @@ void reset_schedule_dev(DeviceCsr &csr, cudaStream_t s)
     check_launch("k_reset_sched");
 }
 
-umapcu_status build_csr_dev(uint32_t n, const uint64_t *d_adj_ptr, const uint32_t *d_adj_col,
-                            const float *d_adj_w, uint64_t nnz, DeviceCsr &csr, cudaStream_t s)
+// One graph's CSR in two phases, so that the structure can be built while
+// the weights are still on their way to the device.
+//
+// Structure (row pointers and columns): flags of the i < j entries, their
+// scan, the edges' endpoints and adjacency positions, the endpoint records
+// (node, 2e + side) stably sorted by node -- each node's entries in
+// ascending edge index, as from_graph lists them -- the offsets, and per
+// entry its other endpoint and edge.
+__global__ void k_edges_struct(const uint32_t *__restrict__ src_row, const uint32_t *__restrict__ adj_col,
+                               const uint32_t *__restrict__ flag, const uint32_t *__restrict__ pos, uint64_t nnz,
+                               uint32_t *__restrict__ ei, uint32_t *__restrict__ ej, uint32_t *__restrict__ epos)
+{
+    const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= nnz || !flag[p]) return;
+    const uint32_t e = pos[p];
+    ei[e] = src_row[p];
+    ej[e] = adj_col[p];
+    epos[e] = (uint32_t)p;
+}
+
+__global__ void k_edge_keys(const uint32_t *__restrict__ ei, const uint32_t *__restrict__ ej, uint64_t E,
+                            uint32_t *__restrict__ key, uint32_t *__restrict__ val, uint32_t *__restrict__ degree)
+{
+    const uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= E) return;
+    const uint32_t a = ei[e], b = ej[e];
+    key[2 * e] = a;
+    val[2 * e] = (uint32_t)(2 * e);
+    key[2 * e + 1] = b;
+    val[2 * e + 1] = (uint32_t)(2 * e + 1);
+    atomicAdd(&degree[a], 1u);
+    atomicAdd(&degree[b], 1u);
+}
+
+__global__ void k_csr_struct(const uint32_t *__restrict__ val_s, uint64_t tot, const uint32_t *__restrict__ ei,
+                             const uint32_t *__restrict__ ej, uint32_t *__restrict__ other,
+                             uint32_t *__restrict__ edge_id)
+{
+    const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= tot + 8) return;
+    if (p >= tot) {
+        other[p] = 0;  // padding behind the last entry, copied (never used) by 16-byte chunk copies
+        return;
+    }
+    const uint32_t v = val_s[p], e = v >> 1;
+    other[p] = (v & 1) ? ei[e] : ej[e];
+    edge_id[p] = e;
+}
+
+// Weights: each edge's weight from its upper entry (mu), the largest from 0
+// (umap_optimiser_gpu.rs:180-184), the periods (:186-196: 1 / (w / max_w),
+// 1e8 when the normalised weight is not positive), and per entry its
+// schedule (cursor = period) and weight, read from one packed (period,
+// weight) pair per edge.
+__global__ void k_edge_weight(const uint32_t *__restrict__ epos, const float *__restrict__ adj_w, uint64_t E,
+                              float *__restrict__ mu)
+{
+    const uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < E) mu[e] = adj_w[epos[e]];
+}
+
+__global__ void k_edge_period(const float *__restrict__ mu, uint64_t E, const float *__restrict__ d_max,
+                              float *__restrict__ eps, float2 *__restrict__ pw)
+{
+    const uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= E) return;
+    const float w = mu[e], norm = w / d_max[0];
+    const float per = norm > 0.0f ? 1.0f / norm : 1e8f;
+    eps[e] = per;
+    pw[e] = make_float2(per, w);
+}
+
+__global__ void k_csr_weights(const uint32_t *__restrict__ edge_id, uint64_t tot, const float2 *__restrict__ pw,
+                              float2 *__restrict__ sched, float *__restrict__ mu_entry)
+{
+    const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= tot + 8) return;
+    if (p >= tot) {
+        sched[p] = make_float2(__int_as_float(0x7f800000), 0.0f);  // padding, never active
+        return;
+    }
+    const float2 q = pw[edge_id[p]];
+    sched[p] = make_float2(q.x, q.x);
+    mu_entry[p] = q.y;
+}
+
+umapcu_status build_csr_structure(uint32_t n, const uint64_t *d_adj_ptr, const uint32_t *d_adj_col, uint64_t nnz,
+                                  DeviceCsr &csr, CsrBuild &tmp, cudaStream_t s)
 {
     if (n == 0) return UMAPCU_NO_DATA;
     if (nnz >= (1ull << 31)) fail(UMAPCU_BAD_ARG, "graph too large for 32-bit CSR entries");
@@ -441,51 +527,72 @@ umapcu_status build_csr_dev(uint32_t n, const uint64_t *d_adj_ptr, const uint32_
         check_launch("k_upper_flags");
     }
     uint32_t bad_h = 0;
-    uint64_t E = scan_flags(flag.p, pos.p, nnz, s, bad.p, &bad_h);
+    const uint64_t E = scan_flags(flag.p, pos.p, nnz, s, bad.p, &bad_h);
     if (bad_h) return UMAPCU_BAD_ARG;
     if (E == 0) return UMAPCU_NO_GRAPH_EDGES;
     csr.n_edges = E;
     DevBuf<uint32_t> ei(E, s), ej(E, s);
-    csr.mu.alloc(E, s);
-    k_edges<<<ceil_div(nnz, 256), 256, 0, s>>>(src_row.p, d_adj_col, d_adj_w, flag.p, pos.p, nnz, ei.p, ej.p,
-                                               csr.mu.p);
-    check_launch("k_edges");
+    tmp.epos.alloc(E, s);
+    k_edges_struct<<<ceil_div(nnz, 256), 256, 0, s>>>(src_row.p, d_adj_col, flag.p, pos.p, nnz, ei.p, ej.p,
+                                                      tmp.epos.p);
+    check_launch("k_edges_struct");
     src_row.release(); flag.release(); pos.release();
-    DevBuf<float> dmax(1, s);
-    reduce_max0(csr.mu.p, E, dmax.p, s);
     const uint64_t tot = 2 * E;
-    csr.eps.alloc(E, s);
     DevBuf<uint32_t> key(tot, s), val(tot, s), key_s(tot, s), val_s(tot, s), degree(n + 1, s);
     check_cuda(cudaMemsetAsync(degree.p, 0, sizeof(uint32_t) * (n + 1), s), "memset");
-    k_edge_records<<<ceil_div(E, 256), 256, 0, s>>>(ei.p, ej.p, csr.mu.p, E, dmax.p, csr.eps.p, key.p, val.p,
-                                                    degree.p, nullptr);
-    check_launch("k_edge_records");
-    int end_bit = bits_for(n);
+    k_edge_keys<<<ceil_div(E, 256), 256, 0, s>>>(ei.p, ej.p, E, key.p, val.p, degree.p);
+    check_launch("k_edge_keys");
+    const int end_bit = bits_for(n);
     size_t tb = 0;
     check_cuda(cub::DeviceRadixSort::SortPairs(nullptr, tb, key.p, key_s.p, val.p, val_s.p, (int64_t)tot, 0,
                                                end_bit, s), "sort size");
     {
-        DevBuf<char> tmp(tb ? tb : 1, s);
-        check_cuda(cub::DeviceRadixSort::SortPairs(tmp.p, tb, key.p, key_s.p, val.p, val_s.p, (int64_t)tot, 0,
+        DevBuf<char> t(tb ? tb : 1, s);
+        check_cuda(cub::DeviceRadixSort::SortPairs(t.p, tb, key.p, key_s.p, val.p, val_s.p, (int64_t)tot, 0,
                                                    end_bit, s), "sort");
     }
+    key.release(); val.release(); key_s.release();
     csr.offsets.alloc(n + 1, s);
     {
         size_t tb2 = 0;
         check_cuda(cub::DeviceScan::ExclusiveSum(nullptr, tb2, degree.p, csr.offsets.p, (int64_t)(n + 1), s),
                    "scan size");
-        DevBuf<char> tmp(tb2 ? tb2 : 1, s);
-        check_cuda(cub::DeviceScan::ExclusiveSum(tmp.p, tb2, degree.p, csr.offsets.p, (int64_t)(n + 1), s),
-                   "scan");
+        DevBuf<char> t(tb2 ? tb2 : 1, s);
+        check_cuda(cub::DeviceScan::ExclusiveSum(t.p, tb2, degree.p, csr.offsets.p, (int64_t)(n + 1), s), "scan");
     }
     csr.other.alloc(tot + 8, s);
     csr.edge_id.alloc(tot, s);
+    k_csr_struct<<<ceil_div(tot + 8, 256), 256, 0, s>>>(val_s.p, tot, ei.p, ej.p, csr.other.p, csr.edge_id.p);
+    check_launch("k_csr_struct");
+    return UMAPCU_OK;
+}
+
+void build_csr_weights(const float *d_adj_w, DeviceCsr &csr, CsrBuild &tmp, cudaStream_t s)
+{
+    const uint64_t E = csr.n_edges, tot = 2 * E;
+    csr.mu.alloc(E, s);
+    csr.eps.alloc(E, s);
     csr.sched.alloc(tot + 8, s);
     csr.mu_entry.alloc(tot, s);
-    k_csr_entries<<<ceil_div(tot + 8, 256), 256, 0, s>>>(val_s.p, tot, ei.p, ej.p, csr.mu.p, csr.eps.p, csr.other.p,
-                                                         csr.edge_id.p, csr.sched.p, csr.mu_entry.p, nullptr,
-                                                         nullptr);
-    check_launch("k_csr_entries");
+    k_edge_weight<<<ceil_div(E, 256), 256, 0, s>>>(tmp.epos.p, d_adj_w, E, csr.mu.p);
+    check_launch("k_edge_weight");
+    tmp.epos.release();
+    DevBuf<float> dmax(1, s);
+    reduce_max0(csr.mu.p, E, dmax.p, s);
+    DevBuf<float2> pw(E, s);
+    k_edge_period<<<ceil_div(E, 256), 256, 0, s>>>(csr.mu.p, E, dmax.p, csr.eps.p, pw.p);
+    check_launch("k_edge_period");
+    k_csr_weights<<<ceil_div(tot + 8, 256), 256, 0, s>>>(csr.edge_id.p, tot, pw.p, csr.sched.p, csr.mu_entry.p);
+    check_launch("k_csr_weights");
+}
+
+umapcu_status build_csr_dev(uint32_t n, const uint64_t *d_adj_ptr, const uint32_t *d_adj_col,
+                            const float *d_adj_w, uint64_t nnz, DeviceCsr &csr, cudaStream_t s)
+{
+    CsrBuild tmp;
+    const umapcu_status rc = build_csr_structure(n, d_adj_ptr, d_adj_col, nnz, csr, tmp, s);
+    if (rc != UMAPCU_OK) return rc;
+    build_csr_weights(d_adj_w, csr, tmp, s);
     return UMAPCU_OK;
 }
 

@@ -102,6 +102,19 @@ struct Stream {
     Stream &operator=(const Stream &) = delete;
 };
 
+// RAII event without timing: ordering between streams.
+struct Event {
+    cudaEvent_t e = nullptr;
+    Event() { check_cuda(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate"); }
+    ~Event()
+    {
+        if (e) cudaEventDestroy(e);
+    }
+    Event(const Event &) = delete;
+    Event &operator=(const Event &) = delete;
+    void record(cudaStream_t s) { check_cuda(cudaEventRecord(e, s), "cudaEventRecord"); }
+};
+
 template <typename T>
 inline void h2d(T *dst, const T *src, size_t count, cudaStream_t s)
 {
@@ -184,6 +197,18 @@ struct DeviceCsr {
 umapcu_status build_csr_dev(uint32_t n, const uint64_t *d_adj_ptr, const uint32_t *d_adj_col,
                             const float *d_adj_w, uint64_t nnz, DeviceCsr &csr, cudaStream_t s);
 
+// The same build in two phases: the structure needs only the row pointers
+// and columns (everything but the weights, periods and schedule), so it can
+// run while the weights are still being copied; the weights phase then
+// completes the CSR. `tmp` carries the edges' adjacency positions between
+// the two.
+struct CsrBuild {
+    DevBuf<uint32_t> epos;  // [E] adjacency position of each edge's upper entry
+};
+umapcu_status build_csr_structure(uint32_t n, const uint64_t *d_adj_ptr, const uint32_t *d_adj_col, uint64_t nnz,
+                                  DeviceCsr &csr, CsrBuild &tmp, cudaStream_t s);
+void build_csr_weights(const float *d_adj_w, DeviceCsr &csr, CsrBuild &tmp, cudaStream_t s);
+
 // Several graphs built as one (the served form's admission). The graphs'
 // adjacencies are concatenated: lptr holds each graph's own row pointers
 // (graph t's n_t + 1 entries start at lptr + node_base[t] + t, counting from
@@ -243,6 +268,12 @@ struct ScheduleBits {
     cudaStream_t built_on = nullptr;  // synchronised before the block goes back to the cache
     uint64_t words = 0;
     uint32_t n_epochs = 0;
+    // Epochs [first, n_epochs) are written on `side` and complete with
+    // `rest` (first = 0: all on built_on); users wait for `rest` before
+    // epoch `first`.
+    uint32_t first = 0;
+    cudaStream_t side = nullptr;
+    cudaEvent_t rest = nullptr;
     ScheduleBits() = default;
     ScheduleBits(const ScheduleBits &) = delete;
     ScheduleBits &operator=(const ScheduleBits &) = delete;
@@ -257,10 +288,13 @@ void release_cached_bits();
 // false when they would not fit (half the free device memory), `out` then
 // empty.
 bool build_schedule_bits(const DeviceCsr &csr, uint32_t n_epochs, ScheduleBits &out, cudaStream_t s);
+// Epochs whose bit words build_schedule_bits writes before the rest.
+constexpr uint32_t kBitsFirst = 8;
 // The bitmask kernel alone: bits [n_epochs][ceil(n_entries / 32)] of the
-// entries' reset schedule (sched[p].y = period), into caller memory.
+// entries' reset schedule (sched[p].y = period), into caller memory; only
+// the words of epochs [e_begin, n_epochs) are written.
 void launch_schedule_bits(const float2 *sched, uint64_t n_entries, uint32_t n_epochs, uint32_t *bits,
-                          cudaStream_t s);
+                          cudaStream_t s, uint32_t e_begin = 0);
 
 // Writes into csr.sched the cursors after `epochs` epochs from the reset
 // schedule (the state the per-epoch scan would have left).

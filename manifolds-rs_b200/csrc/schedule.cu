@@ -142,9 +142,12 @@ __global__ void __launch_bounds__(kSchedWarps * 32) k_sched_lists(const uint32_t
 }
 
 // Bitmasks: thread per 32-entry word, the word's cursors and periods in
-// registers, one word written per epoch (coalesced across the warp).
+// registers, one word written per epoch (coalesced across the warp). The
+// walk starts from the reset schedule and writes the words of epochs
+// [e_begin, n_epochs) only, so a run's epochs can be built in two launches.
 __global__ void __launch_bounds__(128) k_sched_bits(const float2 *__restrict__ sched, uint64_t n_entries,
-                                                    uint64_t words, uint32_t n_epochs, uint32_t *__restrict__ bits)
+                                                    uint64_t words, uint32_t e_begin, uint32_t n_epochs,
+                                                    uint32_t *__restrict__ bits)
 {
     const uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (w >= words) return;
@@ -164,7 +167,7 @@ __global__ void __launch_bounds__(128) k_sched_bits(const float2 *__restrict__ s
             if (a) cur[t] = cur[t] + per[t];
             word |= (a ? 1u : 0u) << t;
         }
-        bits[(size_t)e * words + w] = word;
+        if (e >= e_begin) bits[(size_t)e * words + w] = word;
     }
 }
 
@@ -300,6 +303,16 @@ void ScheduleBits::release()
 {
     if (!bits) return;
     if (built_on) cudaStreamSynchronize(built_on);
+    if (side) {
+        cudaStreamSynchronize(side);
+        cudaStreamDestroy(side);
+        side = nullptr;
+    }
+    if (rest) {
+        cudaEventDestroy(rest);
+        rest = nullptr;
+    }
+    first = 0;
     {
         std::lock_guard<std::mutex> lk(g_bits_mu);
         if (dev >= 0 && dev < 64 && !g_bits_cache[dev].p) {
@@ -328,11 +341,11 @@ void release_cached_bits()
 }
 
 void launch_schedule_bits(const float2 *sched, uint64_t n_entries, uint32_t n_epochs, uint32_t *bits,
-                          cudaStream_t s)
+                          cudaStream_t s, uint32_t e_begin)
 {
     const uint64_t words = (n_entries + 31) / 32;
-    if (!words || !n_epochs) return;
-    k_sched_bits<<<ceil_div(words, 128), 128, 0, s>>>(sched, n_entries, words, n_epochs, bits);
+    if (!words || e_begin >= n_epochs) return;
+    k_sched_bits<<<ceil_div(words, 128), 128, 0, s>>>(sched, n_entries, words, e_begin, n_epochs, bits);
     check_launch("k_sched_bits");
 }
 
@@ -369,9 +382,24 @@ bool build_schedule_bits(const DeviceCsr &csr, uint32_t n_epochs, ScheduleBits &
     out.cap = blk.cap;
     out.dev = dev;
     out.built_on = s;
-    launch_schedule_bits(csr.sched.p, entries, n_epochs, out.bits, s);
     out.words = words;
     out.n_epochs = n_epochs;
+    // The first kBitsFirst epochs' words on s, the rest on a side stream
+    // that starts after them: the run's first epochs then overlap the build
+    // of the later words (run_epoch waits for out.rest before epoch
+    // kBitsFirst).
+    if (n_epochs <= 2 * kBitsFirst) {
+        launch_schedule_bits(csr.sched.p, entries, n_epochs, out.bits, s);
+        return true;
+    }
+    launch_schedule_bits(csr.sched.p, entries, kBitsFirst, out.bits, s);
+    check_cuda(cudaStreamCreateWithFlags(&out.side, cudaStreamNonBlocking), "cudaStreamCreate");
+    check_cuda(cudaEventCreateWithFlags(&out.rest, cudaEventDisableTiming), "cudaEventCreate");
+    check_cuda(cudaEventRecord(out.rest, s), "cudaEventRecord");
+    check_cuda(cudaStreamWaitEvent(out.side, out.rest, 0), "cudaStreamWaitEvent");
+    launch_schedule_bits(csr.sched.p, entries, n_epochs, out.bits, out.side, kBitsFirst);
+    check_cuda(cudaEventRecord(out.rest, out.side), "cudaEventRecord");
+    out.first = kBitsFirst;
     return true;
 }
 
