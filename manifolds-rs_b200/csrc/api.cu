@@ -150,8 +150,11 @@ void run_epoch(umapcu_state *st, uint32_t epoch, uint32_t optimiser, const uint3
     } else if (use_bits) {
         A.bits = st->bits.bits + (size_t)epoch * st->bits.words;
         st->sched_lazy = true;
-        if (st->bits.rest && epoch >= st->bits.first)  // the later epochs' words (build_schedule_bits)
+        if (st->bits.rest && epoch >= st->bits.first && st->bits.waited != st->stream.s) {
+            // the later epochs' words (build_schedule_bits): once per stream
             check_cuda(cudaStreamWaitEvent(st->stream.s, st->bits.rest, 0), "cudaStreamWaitEvent");
+            st->bits.waited = st->stream.s;
+        }
     }
     if (in_order) st->sched_epoch = epoch + 1;
     A.n = st->n;
@@ -230,10 +233,16 @@ umapcu_status create_state(const float *embd, uint32_t n, uint32_t n_dim, const 
     st->p = *params;
     st->seed = seed;
     st->sampler = sampler;
+    const uint64_t nt = (uint64_t)n * n_dim;
+    st->y[0].alloc(nt, s);
+    st->y[1].alloc(nt, s);
+    st->m.alloc(nt, s);
+    st->v.alloc(nt, s);
     {
-        // The row pointers and columns go first; the weights follow on a
-        // second stream while the CSR's structure is built from the former
-        // (build_csr_structure), and the weights phase waits for them.
+        // The row pointers and columns go first; the weights (then the
+        // embedding) follow on a second stream while the CSR's structure is
+        // built from the former (build_csr_structure), and the weights phase
+        // waits for them.
         NvtxRange r("umapcu graph upload + CSR build");
         DevBuf<uint64_t> dptr(n + 1, s);
         DevBuf<uint32_t> dcol(nnz, s);
@@ -245,6 +254,7 @@ umapcu_status create_state(const float *embd, uint32_t n, uint32_t n_dim, const 
         col_in.record(s);
         check_cuda(cudaStreamWaitEvent(side.s, col_in.e, 0), "cudaStreamWaitEvent");
         h2d(dw.p, adj_w, nnz, side.s);
+        h2d(st->y[0].p, embd, nt, side.s);
         w_in.record(side.s);
         CsrBuild tmp;
         const umapcu_status rc = build_csr_structure(n, dptr.p, dcol.p, nnz, st->csr, tmp, s);
@@ -275,12 +285,6 @@ umapcu_status create_state(const float *embd, uint32_t n, uint32_t n_dim, const 
     }
     st->err.alloc(1, s);
     check_cuda(cudaMemsetAsync(st->err.p, 0, sizeof(uint32_t), s), "memset err");
-    const uint64_t nt = (uint64_t)n * n_dim;
-    st->y[0].alloc(nt, s);
-    st->y[1].alloc(nt, s);
-    st->m.alloc(nt, s);
-    st->v.alloc(nt, s);
-    h2d(st->y[0].p, embd, nt, s);
     check_cuda(cudaMemsetAsync(st->m.p, 0, nt * sizeof(float), s), "memset m");
     check_cuda(cudaMemsetAsync(st->v.p, 0, nt * sizeof(float), s), "memset v");
     if (dens) {

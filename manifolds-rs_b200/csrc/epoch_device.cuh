@@ -214,17 +214,18 @@ __device__ __forceinline__ float dens_weight(float r, float re, const float *__r
 // Per-warp shared memory of the segment walk. The queue holds the CSR
 // positions (and, for the cursor scan, the other endpoints) of active
 // entries not yet evaluated: one super-chunk plus the carried partial batch
-// for the cursor scan; for the bitmask scan, a group of 256 entries (a lane
-// per 8) plus the carried partial batch. The densMAP node records only in
-// the densMAP kernels.
-// Shared memory is kept small on purpose: the random coordinate gathers hold
-// their in-flight misses in L1, which gets what the blocks' shared memory
-// leaves of each SM's 256 KB; at 8 resident blocks, 22.6 KB of shared memory
-// per block (a 1024-entry queue) left 60 KB of L1 and 25.8 KB left 28 KB,
-// and the epoch took 141 and 243 us at 1M points.
-template <int D, int KU = kU, bool BITS = false, bool DENS = true>
+// for the cursor scan; for the bitmask scan, a group of 32 x BP entries (a
+// lane per BP) plus the carried partial batch. The densMAP node records only
+// in the densMAP kernels.
+// Shared memory is sized with care: the random coordinate gathers hold their
+// in-flight misses in L1, which gets what the blocks' shared memory leaves of
+// each SM's 256 KB; at 8 resident blocks, 22.6 KB of shared memory per block
+// (a 1024-entry queue) left 60 KB of L1 and 25.8 KB left 28 KB, and the epoch
+// took 141 and 243 us at 1M points. Larger groups cost less per entry on
+// long segments, smaller ones leave more L1 (bits_piece).
+template <int D, int KU = kU, bool BITS = false, bool DENS = true, int BP = 32>
 struct WarpSmem {
-    static constexpr int kQ = BITS ? 8 * 32 + 32 : 32 * KU + 32;
+    static constexpr int kQ = BITS ? BP * 32 + 32 : 32 * KU + 32;
     uint32_t beg[33];
     uint32_t qp[kQ];
     uint32_t qo[BITS ? 1 : kQ];
@@ -469,8 +470,8 @@ __device__ __forceinline__ void finish_node(const EpochArgs &A, uint32_t node, c
 // BITS: the scan reads the epoch's active-entry bitmask (A.bits) in place of
 // the entries' (cursor, period) and writes no cursor.
 template <int D, bool DENS, int NR, bool COH, int KU = kU, bool FAST = false, bool LIST = false,
-          bool BITS = false>
-__device__ __forceinline__ void epoch_segment(const EpochArgs &A, WarpSmem<D, KU, BITS, DENS> &S, uint32_t node0,
+          bool BITS = false, int BP = 32>
+__device__ __forceinline__ void epoch_segment(const EpochArgs &A, WarpSmem<D, KU, BITS, DENS, BP> &S, uint32_t node0,
                                               int lane)
 {
     __syncwarp();  // the warp's shared memory may still be read by its previous segment
@@ -504,8 +505,8 @@ __device__ __forceinline__ void epoch_segment(const EpochArgs &A, WarpSmem<D, KU
             process_batch<D, DENS, NR, COH, KU, FAST>(A, S, live, p, o, j, el, node0, lane, g, act, dstat, S.part);
         }
     } else if constexpr (BITS) {
-        // The epoch's bit words in pieces of 8 CSR entries, a lane per piece,
-        // 256 entries at a time: the pieces are masked to the segment, an
+        // The epoch's bit words in pieces of BP CSR entries, a lane per piece,
+        // 32 x BP entries at a time: the pieces are masked to the segment, an
         // exclusive warp prefix of their popcounts gives each lane its first
         // queue slot, and each lane writes the positions of its set bits in
         // ascending order -- so the queue holds the active entries in CSR
@@ -514,14 +515,16 @@ __device__ __forceinline__ void epoch_segment(const EpochArgs &A, WarpSmem<D, KU
         // one batch ahead.
         const uint32_t seg_beg = S.beg[0], seg_end = S.beg[32];
         uint32_t count = 0;
-        for (uint64_t e0 = seg_beg & ~7u; e0 < seg_end; e0 += 256u) {
-            const uint64_t wb = e0 + 8u * (uint32_t)lane;
+        static_assert(BP == 8 || BP == 16 || BP == 32, "pieces of 8, 16 or 32 entries");
+        for (uint64_t e0 = seg_beg & ~(uint32_t)(BP - 1); e0 < seg_end; e0 += 32u * BP) {
+            const uint64_t wb = e0 + (uint32_t)BP * (uint32_t)lane;
             uint32_t m = 0;
             if (wb < seg_end) {
-                // the piece lies inside one word: wb is a multiple of 8
-                m = (__ldg(A.bits + (wb >> 5)) >> ((uint32_t)wb & 31u)) & 0xFFu;
-                if (wb < seg_beg) m &= 0xFFu << (seg_beg - (uint32_t)wb);
-                if (seg_end - wb < 8u) m &= (1u << (uint32_t)(seg_end - wb)) - 1u;
+                // the piece lies inside one word: wb is a multiple of BP
+                const uint32_t word = __ldg(A.bits + (wb >> 5));
+                m = BP == 32 ? word : (word >> ((uint32_t)wb & 31u)) & ((1u << (BP & 31)) - 1u);
+                if (wb < seg_beg) m &= ~0u << (seg_beg - (uint32_t)wb);
+                if (seg_end - wb < (uint32_t)BP) m &= (1u << (uint32_t)(seg_end - wb)) - 1u;
             }
             const uint32_t c = __popc(m);
             uint32_t x = c;
@@ -537,7 +540,7 @@ __device__ __forceinline__ void epoch_segment(const EpochArgs &A, WarpSmem<D, KU
             }
             count += __shfl_sync(kFull, x, 31);
             __syncwarp();
-            const bool last = e0 + 256u >= seg_end;
+            const bool last = e0 + 32u * BP >= seg_end;
             const uint32_t upto = last ? count : (count & ~31u);
             uint32_t p = 0, o = 0;
             if ((uint32_t)lane < upto) {
@@ -723,7 +726,7 @@ constexpr uint32_t kSplitWords = 256;
 // bit. Partials are added in batch order as in epoch_segment_split, so the
 // result is bit-identical to the scan.
 template <int D, bool DENS, int NR, bool FAST>
-__device__ __forceinline__ void epoch_segment_split_bits(const EpochArgs &A, WarpSmem<D, kU, true, DENS> &S,
+__device__ __forceinline__ void epoch_segment_split_bits(const EpochArgs &A, WarpSmem<D, kU, true, DENS, 32> &S,
                                                          float (*part)[32][D],
                                                          unsigned *has_w, uint32_t *wm, uint32_t *pre,
                                                          uint32_t node0, int warp, int lane)

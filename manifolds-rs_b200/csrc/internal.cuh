@@ -274,6 +274,7 @@ struct ScheduleBits {
     uint32_t first = 0;
     cudaStream_t side = nullptr;
     cudaEvent_t rest = nullptr;
+    cudaStream_t waited = nullptr;  // the stream that last waited for `rest`
     ScheduleBits() = default;
     ScheduleBits(const ScheduleBits &) = delete;
     ScheduleBits &operator=(const ScheduleBits &) = delete;
@@ -288,8 +289,11 @@ void release_cached_bits();
 // false when they would not fit (half the free device memory), `out` then
 // empty.
 bool build_schedule_bits(const DeviceCsr &csr, uint32_t n_epochs, ScheduleBits &out, cudaStream_t s);
-// Epochs whose bit words build_schedule_bits writes before the rest.
+// Epochs whose bit words build_schedule_bits writes before the rest, for
+// bitmasks of at least kBitsSplitWords words (64 MB; smaller ones are built
+// in one launch).
 constexpr uint32_t kBitsFirst = 8;
+constexpr size_t kBitsSplitWords = (size_t)16 << 20;
 // The bitmask kernel alone: bits [n_epochs][ceil(n_entries / 32)] of the
 // entries' reset schedule (sched[p].y = period), into caller memory; only
 // the words of epochs [e_begin, n_epochs) are written.

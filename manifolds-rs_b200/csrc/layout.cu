@@ -43,11 +43,24 @@
 
 namespace umapcu {
 
+// Resident blocks per SM the register budget is set for: 10 (48 registers,
+// 40 warps) for the fast path in one or two dimensions without the density
+// term, whose gathers then keep more misses in flight; 6 elsewhere, where 48
+// registers would spill.
+template <int D, bool DENS, bool FAST>
+constexpr int epoch_min_blocks() { return FAST && !DENS && D <= 2 ? 10 : 6; }
+// Entries per lane of the bitmask scan's groups: 16 in the kernels run at 10
+// blocks per SM (7.3 KB of shared memory per block at 8, 11.4 KB at 16, so
+// that L1 keeps ~130 KB), 32 -- a bit word per lane, the fewest groups on
+// long segments -- elsewhere.
+template <int D, bool DENS, bool FAST>
+constexpr int bits_piece() { return FAST && !DENS && D <= 2 ? 16 : 32; }
+
 template <int D, bool DENS, int NR, bool FAST = false, bool LIST = false, bool BITS = false>
-__global__ void __launch_bounds__(kWarps * 32, 6) k_epoch(const EpochArgs A)
+__global__ void __launch_bounds__(kWarps * 32, epoch_min_blocks<D, DENS, FAST>()) k_epoch(const EpochArgs A)
 {
     constexpr int KU = LIST ? 1 : kU;  // the list path keeps no scan queue
-    __shared__ WarpSmem<D, KU, BITS, DENS> smem[kWarps];
+    __shared__ WarpSmem<D, KU, BITS, DENS, bits_piece<D, DENS, FAST>()> smem[kWarps];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t node0 = (blockIdx.x * kWarps + warp) * 32u;
     if (node0 >= A.n) return;

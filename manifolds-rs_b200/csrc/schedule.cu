@@ -313,6 +313,7 @@ void ScheduleBits::release()
         rest = nullptr;
     }
     first = 0;
+    waited = nullptr;
     {
         std::lock_guard<std::mutex> lk(g_bits_mu);
         if (dev >= 0 && dev < 64 && !g_bits_cache[dev].p) {
@@ -388,7 +389,7 @@ bool build_schedule_bits(const DeviceCsr &csr, uint32_t n_epochs, ScheduleBits &
     // that starts after them: the run's first epochs then overlap the build
     // of the later words (run_epoch waits for out.rest before epoch
     // kBitsFirst).
-    if (n_epochs <= 2 * kBitsFirst) {
+    if (n_epochs <= 2 * kBitsFirst || need < kBitsSplitWords) {
         launch_schedule_bits(csr.sched.p, entries, n_epochs, out.bits, s);
         return true;
     }
