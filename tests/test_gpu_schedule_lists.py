@@ -159,6 +159,32 @@ def test_one_shot_bitmask_warp_per_segment_equals_scan():
     assert np.array_equal(_one_shot(adj, emb, p), _one_shot(adj, emb, p, precompute=False))
 
 
+def test_split_bitmask_build_equals_scan():
+    """Bitmasks of 64 MB or more are built in two launches, epochs 8.. on a
+    side stream beside the first epochs, which wait for it once before epoch
+    8 (here 200k points, ~4.7 M CSR entries, 150 epochs: ~88 MB). The
+    one-shot call and a resident state that switches to the bitmask form
+    mid-life (its epochs on another stream) equal the cursor scan bit for
+    bit."""
+    import torch
+    import umapdata.synth as S
+    n = 200_000
+    X, _ = S.isotropic_mixture(n, 16, 12, 6)
+    idx, dist = umapcu.knn_exact(X, 15)
+    adj = umapcu.coo_to_adjacency_list(umapcu.construct_umap_graph(idx, dist, umapcu.UmapGraphParams(), 150))
+    p = umapcu.UmapOptimParams(n_epochs=150)
+    assert 150 * ((int(adj.ptr[-1]) + 31) // 32) >= 16 << 20  # takes the split build
+    emb = init_embedding(n, 2, seed=15)
+    y_scan = _one_shot(adj, emb, p, precompute=False)
+    assert np.array_equal(_one_shot(adj, emb, p), y_scan)
+    st = _state(adj, emb, p, False)
+    st.set_schedule(umapcu.SCHED_BITS)
+    st.set_stream(torch.cuda.current_stream().cuda_stream)
+    st.run(0, 150)
+    assert np.array_equal(st.read()[0], y_scan)
+    st.close()
+
+
 def test_one_shot_bitmask_hub_segment_equals_scan():
     """A hub with 9000 neighbours puts more than 256 bitmask words into one
     segment: that segment runs the sequential scan on one warp while the
