@@ -86,7 +86,9 @@ __device__ __forceinline__ bool checked_ok(bool ok, uint32_t *err)
 // L2 residency: the embedding (gathered at random every epoch) is loaded
 // with an evict_last policy; the CSR arrays (streamed once per epoch) with
 // the streaming (evict-first) qualifier, so they do not push the embedding
-// out of L2.
+// out of L2. The random gathers do not allocate in L1 (they almost never
+// hit there), which leaves L1 to the segment's streamed lines (1M points:
+// 26.5 -> 26.1 ms per 200-epoch run).
 __device__ __forceinline__ uint64_t l2_keep_policy()
 {
     uint64_t pol;
@@ -108,7 +110,7 @@ __device__ __forceinline__ void load_row_keep(const float *__restrict__ y, uint3
                          : "=f"(out[0]), "=f"(out[1])
                          : "l"(a), "l"(pol));
         else
-            asm volatile("ld.global.nc.L2::cache_hint.v2.f32 {%0, %1}, [%2], %3;"
+            asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.f32 {%0, %1}, [%2], %3;"
                          : "=f"(out[0]), "=f"(out[1])
                          : "l"(a), "l"(pol));
     } else if constexpr (D == 4) {
@@ -118,7 +120,7 @@ __device__ __forceinline__ void load_row_keep(const float *__restrict__ y, uint3
                          : "=f"(out[0]), "=f"(out[1]), "=f"(out[2]), "=f"(out[3])
                          : "l"(a), "l"(pol));
         else
-            asm volatile("ld.global.nc.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+            asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
                          : "=f"(out[0]), "=f"(out[1]), "=f"(out[2]), "=f"(out[3])
                          : "l"(a), "l"(pol));
     } else {
@@ -128,7 +130,7 @@ __device__ __forceinline__ void load_row_keep(const float *__restrict__ y, uint3
             if constexpr (COH)
                 asm volatile("ld.global.cg.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(out[d]) : "l"(a), "l"(pol));
             else
-                asm volatile("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(out[d]) : "l"(a), "l"(pol));
+                asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(out[d]) : "l"(a), "l"(pol));
         }
     }
 }
