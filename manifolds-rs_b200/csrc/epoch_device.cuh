@@ -719,6 +719,10 @@ __device__ __forceinline__ uint32_t select_bit(uint32_t m, uint32_t k)
 // Words of a segment's bitmask one block of epoch_segment_split_bits holds;
 // a longer segment runs on warp 0 alone with the sequential scan.
 constexpr uint32_t kSplitWords = 256;
+// Warps of a k_epoch_split_bits block: a small problem's segment has a few
+// batches per epoch, and each warp takes one batch per round, so more warps
+// mean fewer dependent rounds of gathers per epoch.
+constexpr int kSplitBitsWarps = 8;
 
 // The bitmask form of epoch_segment_split: the block reads the segment's
 // words of the epoch's bitmask, masks them to the segment's entries, and
@@ -727,7 +731,7 @@ constexpr uint32_t kSplitWords = 256;
 // lane t finds its entry by searching the prefix counts and selecting the
 // bit. Partials are added in batch order as in epoch_segment_split, so the
 // result is bit-identical to the scan.
-template <int D, bool DENS, int NR, bool FAST>
+template <int D, bool DENS, int NR, bool FAST, int W = kWarps>
 __device__ __forceinline__ void epoch_segment_split_bits(const EpochArgs &A, WarpSmem<D, kU, true, DENS, 32> &S,
                                                          float (*part)[32][D],
                                                          unsigned *has_w, uint32_t *wm, uint32_t *pre,
@@ -778,7 +782,7 @@ __device__ __forceinline__ void epoch_segment_split_bits(const EpochArgs &A, War
 #pragma unroll
     for (int d = 0; d < D; d++) g[d] = 0.0f;
     bool act = false;
-    for (uint32_t r0 = 0; r0 < total; r0 += 32u * kWarps) {  // block-uniform
+    for (uint32_t r0 = 0; r0 < total; r0 += 32u * W) {  // block-uniform
         const uint32_t rb = r0 + 32u * warp;
         unsigned has = 0;
         if (rb < total) {  // warp-uniform
@@ -806,7 +810,7 @@ __device__ __forceinline__ void epoch_segment_split_bits(const EpochArgs &A, War
         __syncthreads();
         if (warp == 0) {
 #pragma unroll
-            for (int w = 0; w < kWarps; w++) {
+            for (int w = 0; w < W; w++) {
                 if ((has_w[w] >> lane) & 1u) {
                     act = true;
 #pragma unroll

@@ -82,14 +82,14 @@ __global__ void __launch_bounds__(kWarps * 32) k_epoch_split(const EpochArgs A)
 // The bitmask form on a small problem: one block per segment, see
 // epoch_segment_split_bits.
 template <int D, bool DENS, int NR, bool FAST>
-__global__ void __launch_bounds__(kWarps * 32) k_epoch_split_bits(const EpochArgs A)
+__global__ void __launch_bounds__(kSplitBitsWarps * 32) k_epoch_split_bits(const EpochArgs A)
 {
     __shared__ WarpSmem<D, kU, true, DENS> seg;
-    __shared__ float part[kWarps][32][D];
-    __shared__ unsigned has_w[kWarps];
+    __shared__ float part[kSplitBitsWarps][32][D];
+    __shared__ unsigned has_w[kSplitBitsWarps];
     __shared__ uint32_t wm[kSplitWords], pre[kSplitWords + 1];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    epoch_segment_split_bits<D, DENS, NR, FAST>(A, seg, part, has_w, wm, pre, blockIdx.x * 32u, warp, lane);
+    epoch_segment_split_bits<D, DENS, NR, FAST, kSplitBitsWarps>(A, seg, part, has_w, wm, pre, blockIdx.x * 32u, warp, lane);
 }
 
 // ------------------------------------------------------------ densMAP
@@ -424,9 +424,9 @@ static void launch_epoch_t(const EpochArgs &A, cudaStream_t s)
         else if (A.neg_rate == 5) k_epoch<D, DENS, 5, false, true><<<grid, kWarps * 32, 0, s>>>(A);
         else k_epoch<D, DENS, 0, false, true><<<grid, kWarps * 32, 0, s>>>(A);
     } else if (A.bits && nseg < kSplitSegments) {
-        if (A.neg_rate == 5 && fast) k_epoch_split_bits<D, DENS, 5, true><<<nseg, kWarps * 32, 0, s>>>(A);
-        else if (A.neg_rate == 5) k_epoch_split_bits<D, DENS, 5, false><<<nseg, kWarps * 32, 0, s>>>(A);
-        else k_epoch_split_bits<D, DENS, 0, false><<<nseg, kWarps * 32, 0, s>>>(A);
+        if (A.neg_rate == 5 && fast) k_epoch_split_bits<D, DENS, 5, true><<<nseg, kSplitBitsWarps * 32, 0, s>>>(A);
+        else if (A.neg_rate == 5) k_epoch_split_bits<D, DENS, 5, false><<<nseg, kSplitBitsWarps * 32, 0, s>>>(A);
+        else k_epoch_split_bits<D, DENS, 0, false><<<nseg, kSplitBitsWarps * 32, 0, s>>>(A);
     } else if (A.bits) {
         if (A.neg_rate == 5 && fast) k_epoch<D, DENS, 5, true, false, true><<<grid, kWarps * 32, 0, s>>>(A);
         else if (A.neg_rate == 5) k_epoch<D, DENS, 5, false, false, true><<<grid, kWarps * 32, 0, s>>>(A);
