@@ -239,47 +239,72 @@ __global__ void __launch_bounds__(kDensBlock) k_dens_update(const DensArgs A)
             const uint32_t p = a + u;
             in[u] = p >= seg_beg && p < seg_end;
             in[u] = in[u] && checked_ok(o[u] < n, A.err);
+#pragma unroll
+            for (int d = 0; d < D; d++) yo[u][d] = 0.0f;
             if (in[u]) load_row_keep<D>(A.y, o[u], yo[u], pol);
         }
         // the next window's endpoints, in flight while this one computes
         if (w0 + kWin < seg_end)
             dens_load_piece<P>(A.other, A.n_entries, vec, a + kWin, seg_beg, seg_end, o);
-        // the piece in CSR order
+        // the piece in CSR order: each entry's node (jj) and that node's
+        // position (ys read when the node changes) ...
         uint32_t j = local_node(S.beg, a);
         const uint32_t j_first = j;
-        uint32_t nxt = S.beg[j + 1];
-        float yj[D];
+        uint32_t jj[P];
+        float yv[P][D];
+        {
+            uint32_t nxt = S.beg[j + 1];
+            float yj[D];
 #pragma unroll
-        for (int d = 0; d < D; d++) yj[d] = S.ys[j][d];
+            for (int d = 0; d < D; d++) yj[d] = S.ys[j][d];
+#pragma unroll
+            for (int u = 0; u < P; u++) {
+                const uint32_t p = a + u;
+                if (in[u] && p >= nxt) {  // a later node's row starts here
+                    do j++;
+                    while (p >= S.beg[j + 1]);
+                    nxt = S.beg[j + 1];
+#pragma unroll
+                    for (int d = 0; d < D; d++) yj[d] = S.ys[j][d];
+                }
+                jj[u] = j;
+#pragma unroll
+                for (int d = 0; d < D; d++) yv[u][d] = yj[d];
+            }
+        }
+        // ... then phi and phi * d^2 of all entries, independent of each other
+        // (no branch: entries outside the segment give 0, which leaves the sums
+        // below unchanged) ...
+        float ph[P], pq[P];
+#pragma unroll
+        for (int u = 0; u < P; u++) {
+            float dist_sq = 0.0f;
+#pragma unroll
+            for (int d = 0; d < D; d++) {
+                const float diff = yv[u][d] - yo[u][d];
+                dist_sq += diff * diff;
+            }
+            const float dist_sq_b = pow_pos(dist_sq, A.b, PRECISE);
+            const float phi = div_k(1.0f, 1.0f + A.a * dist_sq_b, PRECISE);
+            ph[u] = in[u] ? phi : 0.0f;
+            pq[u] = in[u] ? phi * dist_sq : 0.0f;
+        }
+        // ... and the sums per node in CSR order
         float ps = 0.0f, pp = 0.0f;
         float2 hf = make_float2(0.0f, 0.0f);  // the first node's partial, once closed
         bool first = true;
+        uint32_t jc = j_first;
 #pragma unroll
         for (int u = 0; u < P; u++) {
-            const uint32_t p = a + u;
-            if (in[u] && p >= nxt) {  // a later node's row starts here
+            if (jj[u] != jc) {
                 if (first) hf = make_float2(ps, pp);
-                else S.C[j] = make_float2(ps, pp);
+                else S.C[jc] = make_float2(ps, pp);
                 first = false;
                 ps = pp = 0.0f;
-                do j++;
-                while (p >= S.beg[j + 1]);
-                nxt = S.beg[j + 1];
-#pragma unroll
-                for (int d = 0; d < D; d++) yj[d] = S.ys[j][d];
+                jc = jj[u];
             }
-            if (in[u]) {
-                float dist_sq = 0.0f;
-#pragma unroll
-                for (int d = 0; d < D; d++) {
-                    const float diff = yj[d] - yo[u][d];
-                    dist_sq += diff * diff;
-                }
-                const float dist_sq_b = pow_pos(dist_sq, A.b, PRECISE);
-                const float phi = div_k(1.0f, 1.0f + A.a * dist_sq_b, PRECISE);
-                ps += phi * dist_sq;
-                pp += phi;
-            }
+            ps += pq[u];
+            pp += ph[u];
         }
         // this piece's first node's partial (h), and its last node's (t) when
         // that is another node
