@@ -164,6 +164,37 @@ def test_csr_asymmetric_input():
     assert csr["n_edges"] == 2 and csr["offsets"].tolist() == [0, 2, 3, 4]
 
 
+def _adj(rows):
+    ptr = np.zeros(len(rows) + 1, np.uint64)
+    ptr[1:] = np.cumsum([len(r) for r in rows])
+    return ptr, [c for r in rows for c, _ in r], [w for r in rows for _, w in r]
+
+
+def test_csr_other_adjacency_forms():
+    """from_graph (umap_optimiser_gpu.rs:132-209) on the adjacency forms the
+    device build is also tested on, with the results its definition gives:
+    edges are the i < j entries in adjacency order, each node's CSR row lists
+    its edges in edge order, periods are 1 / (w / max_w) or 1e8."""
+    # an unsorted row, and lower entries whose weights differ from their mirrors'
+    st, c = O.csr_from_graph(3, *_adj([[(2, 0.5), (1, 1.0)], [(0, 0.3)], [(0, 0.9), (1, 0.25)]]))
+    assert st == O.OK and c["n_edges"] == 2
+    assert c["offsets"].tolist() == [0, 2, 3, 4]
+    assert c["edge_idx"].tolist() == [0, 1, 1, 0] and c["other"].tolist() == [2, 1, 0, 0]
+    assert c["eps"].tolist() == [2.0, 1.0] and c["mu"].tolist() == [0.5, 1.0]
+    # a repeated entry is a second edge; a self entry is dropped
+    st, c = O.csr_from_graph(2, *_adj([[(0, 1.0), (1, 0.5), (1, 0.5)], [(0, 0.5)]]))
+    assert st == O.OK and c["n_edges"] == 2
+    assert c["offsets"].tolist() == [0, 2, 4]
+    assert c["edge_idx"].tolist() == [0, 1, 0, 1] and c["other"].tolist() == [1, 1, 0, 0]
+    assert c["eps"].tolist() == [1.0, 1.0]
+    # only lower entries: no edge
+    st, _ = O.csr_from_graph(3, *_adj([[], [(0, 0.7)], [(1, 0.4)]]))
+    assert st == O.NO_GRAPH_EDGES
+    # a zero weight gets the 1e8 period
+    st, c = O.csr_from_graph(3, *_adj([[(1, 0.0), (2, 1.0)], [], []]))
+    assert st == O.OK and c["eps"].tolist() == [np.float32(1e8), 1.0]
+
+
 # ------------------------------------------------- kernels (CPU mirrors)
 
 def _tri_params():
